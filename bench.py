@@ -1,0 +1,343 @@
+"""Benchmark: fault x pattern evaluations per second on the 200k-gate workload.
+
+Workload (c2, lsim_b200/gen.py): seeded synthetic circuit with 200,000 gates,
+1,000 PIs, 1,000 POs and 150 levels (mean fan-in 2.2); SA0/SA1 on every gate
+output and input pin, collapsed by equivalence; 65,536 uniform patterns.
+One step simulates every fault against every pattern (count mode) and brings
+the per-fault results back to the host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: device time of K steps with circuit, faults and patterns resident on
+the GPU (CUDA events on the launch stream, max over ranks).
+e2e:   the same through the public API from host buffers: pattern words
+       uploaded from pinned host memory and per-fault results read back every
+       step.
+With N > 1 each rank simulates its own 65,536-pattern block (seed = rank)
+and the per-fault results are merged across ranks every step (weak scaling).
+--impl reference times LSIM's own CPU simulator (oracle/_ref, else the CPU
+port in oracle/) on a bounded sample of the same workload on all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2"
+METRIC = "fault×pattern evals/s (200k-gate)"
+UNIT = "fault-patterns/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_sweep_c2.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_per_launch_bytes:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        self.gpu = vis.split(",")[local_rank] if vis else str(local_rank)
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-i", self.gpu, "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().splitlines() if r.count(",") >= 8]
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _output_fault_sample(flst_text, n):
+    """First n output faults (pin 0) of an @pins list, as plain .flst text."""
+    toks = flst_text.split()
+    pins = toks[0] == "@pins"
+    if pins:
+        toks = toks[1:]
+    F = int(toks[0])
+    out = []
+    step = 3 if pins else 2
+    for i in range(F):
+        site, val = toks[1 + step * i], toks[2 + step * i]
+        pin = toks[3 + step * i] if pins else "0"
+        if pin == "0":
+            out.append("%s %s" % (site, val))
+            if len(out) == n:
+                break
+    return "%d\n%s\n" % (len(out), "\n".join(out))
+
+
+def cpu_baseline(w, target_s=15.0):
+    """The reference simulator (else the CPU port) on a bounded sample of the
+    workload: S output faults x R rounds, all faults sharded over threads."""
+    from tests.oracle_lib import Oracle, Reference, ref_available
+    threads = max(1, min(64, os.cpu_count() or 1))
+    full = Oracle(w["ckt"], "0\n", w["ptn"])
+    if ref_available():
+        kind = "reference"
+        fl = _output_fault_sample(w["flst"], 4 * threads)
+        ref = Reference(w["ckt"], fl, words=full.words, P=full.P, n_pi=full.n_pi)
+        ref.simulate(rd0=0, rd1=1, threads=threads)          # load workers, calibrate
+        per_round = max(ref.seconds, 1e-3)
+        R = int(max(1, min(full.W, target_s / per_round)))
+        ref.simulate(rd0=0, rd1=R, threads=threads)
+        secs, nf = ref.seconds, ref.F
+    else:
+        kind = "port"
+        fl = _output_fault_sample(w["flst"], 32 * threads)
+        o = Oracle(w["ckt"], fl, w["ptn"])
+        t0 = time.perf_counter()
+        o.simulate(rd0=0, rd1=1, mode=0, threads=threads)
+        per_round = max(time.perf_counter() - t0, 1e-3)
+        R = int(max(1, min(full.W, target_s / per_round)))
+        t0 = time.perf_counter()
+        o.simulate(rd0=0, rd1=R, mode=0, threads=threads)
+        secs, nf = time.perf_counter() - t0, len(o.faults)
+    value = nf * R * 64 / secs
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "%d output faults x %d rounds (%d patterns) of the %s workload, %.1f s"
+                      % (nf, R, R * 64, WORKLOAD, secs)}
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    from lsim_b200 import gen
+    w = gen.workload(WORKLOAD)
+    n_faults = int(w["flst"].split()[1 if w["flst"].startswith("@pins") else 0])
+    for _ in range(args.warmup):
+        cpu_baseline(w, target_s=2.0)
+    vals, secs = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b = cpu_baseline(w, target_s=args.ref_seconds)
+        vals.append(b["value"])
+    elapsed = time.perf_counter() - t0
+    value = statistics.median(vals)
+    P = 65536
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * n_faults * P / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": _workload_desc(n_faults), "mode": "count",
+                       "timed": "bounded sample per step; ms_per_step extrapolated to the full job"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": b["cores"], "kind": b["kind"],
+                             "sample": b["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": elapsed}
+    print(json.dumps(line), flush=True)
+
+
+def _workload_desc(n_faults):
+    return ("c2: 200,000 gates, 1,000 PI, 1,000 PO, 150 levels, mean fan-in 2.2; %d collapsed "
+            "output+input-pin SA faults; 65,536 patterns" % n_faults)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from lsim_b200 import Simulator, gen, shard
+
+    w = gen.workload(WORKLOAD, pattern_seed=rank)
+    sim = Simulator(local)
+    sim.read_text(w["ckt"], w["flst"], w["ptn"])
+    info = sim.info()
+    F, P = info.num_faults, info.num_patterns
+    words = sim.patterns()
+    pinned = torch.from_numpy(words.ravel()).pin_memory()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def merge(res):
+        if world == 1:
+            return res
+        return shard.merge_results(res, rank * P, rank == world - 1, world * info.num_rounds,
+                                   device="cuda")
+
+    for _ in range(args.warmup):
+        sim.run(stream=sp)
+        merge(sim.results())
+    torch.cuda.synchronize()
+
+    # value: inputs resident, K steps
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sweep_ms, sweep_bytes, tiles, launches = 0.0, 0, 0, 0
+    for _ in range(args.steps):
+        sim.run(stream=sp)
+        merged = merge(sim.results())
+        st = sim.stats()
+        sweep_ms += st["ms_sweep"]
+        sweep_bytes += st["sweep_alg_bytes"]
+        tiles += st["n_tiles"]
+        launches += st["kernel_launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # e2e: patterns from pinned host memory each step, results back each step
+    host_words = pinned.numpy()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(args.steps):
+        sim.set_patterns(host_words, P)
+        sim.run(stream=sp)
+        merged = merge(sim.results())
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = g0.elapsed_time(g1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    del merged
+
+    units = float(world) * F * P * args.steps
+    value = units / (ms / 1e3)
+    e2e = units / (ms_e2e / 1e3)
+    peak, peak_src = _peaks()
+    per_launch_bytes = sweep_bytes / max(1, tiles)
+    per_launch_s = sweep_ms / max(1, tiles) / 1e3
+    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    st = sim.stats()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": _workload_desc(F), "faults": F, "patterns": P,
+                   "elements": info.num_elements, "mode": "count",
+                   "parallelism": "pattern-sharded x%d" % world if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2: good-machine words %.2f GB rewritten each step"
+                         % (info.num_elements * info.num_rounds * 8 / 1e9),
+                   "sweep": {"words_per_item": st["words_per_item"],
+                             "block_threads": st["block_threads"], "blocks": st["blocks"],
+                             "smem_bytes": st["smem_bytes"], "max_live": st["max_live"]}},
+        "e2e": {"value": e2e, "unit": UNIT,
+                "h2d_bytes_per_step": int(words.nbytes),
+                "d2h_bytes_per_step": int(F * 17)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": _profile_traffic(),
+                     "kernel": "k_sweep", "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "per_launch_alg_bytes": per_launch_bytes, "per_launch_ms": per_launch_s * 1e3},
+        "breakdown_ms_per_step": {"good": st["ms_good"], "sweep": st["ms_sweep"],
+                                  "ffr": st["ms_ffr"], "compute": st["ms_compute"],
+                                  "total": st["ms_total"]},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, target_s=args.ref_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

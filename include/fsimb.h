@@ -1,0 +1,177 @@
+/*
+ * fsimb.h -- C ABI of the B200-native stuck-at fault simulator.
+ *
+ * The library replaces the simulation layer of LSIM (fsim::Simulator,
+ * fsim/simulation.hpp:39-188, and CUDAMAPartitioner,
+ * fsim/cuda_MA_partition/cuda_MA_partition.cuh:125-260) behind plain C entry
+ * points: opaque handle, plain pointers and sizes, an int status on every
+ * call (0 = ok) and a per-handle error message.  No exception and no exit()
+ * crosses this boundary.  A handle is used by one thread at a time;
+ * different handles are independent.  Device memory belongs to the handle.
+ *
+ * Inputs are LSIM's .ckt / .flst / .ptn text formats with the reference's
+ * semantics (element order, fault mapping, pattern rounds).  Results per
+ * fault: detected flag, first detecting pattern (-1 if none), detection
+ * count, and the reference's own last-round view of found_fault_to_pattern.
+ */
+#ifndef FSIMB_H
+#define FSIMB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define FSIMB_OK 0
+#define FSIMB_ERR_ARG 1     /* bad argument or size */
+#define FSIMB_ERR_PARSE 2   /* malformed or unsupported input text */
+#define FSIMB_ERR_CUDA 3    /* CUDA runtime error or no usable GPU */
+#define FSIMB_ERR_STATE 4   /* call order (e.g. results before run) */
+#define FSIMB_ERR_NOMEM 5   /* host or device allocation failed */
+#define FSIMB_ERR_IO 6      /* file could not be opened or read */
+#define FSIMB_ERR_LIMIT 7   /* circuit exceeds a documented limit */
+
+typedef struct fsimb_handle fsimb_handle;
+
+/* One fault's result (32 bytes). */
+typedef struct {
+  uint8_t detected;            /* some pattern detects the fault */
+  uint8_t ref_last_round_flag; /* found_fault_to_pattern[2f] of the reference */
+  uint8_t pad[6];
+  int64_t first_pattern;       /* lowest detecting pattern index, -1 if none */
+  uint64_t count;              /* detecting patterns (count mode) */
+  uint64_t ref_last_rd;        /* found_fault_to_pattern[2f+1] of the reference */
+} fsimb_fault_result;
+
+/* Run options.  Zero-initialise and set struct_size = sizeof(fsimb_opts). */
+typedef struct {
+  uint32_t struct_size;
+  uint32_t drop;             /* 0: count mode (every pattern); 1: drop a fault
+                                after the 2048-pattern tile that first detects
+                                it (first_pattern exact, count covers that tile) */
+  uint32_t words_per_item;   /* sweep words per work item: 0 auto, or 1,2,4,8 */
+  uint32_t block_threads;    /* sweep CTA size: 0 auto, or 32..512 */
+  void* stream;              /* cudaStream_t to run on; NULL: the handle's stream */
+} fsimb_opts;
+
+/* Sizes of the loaded problem. */
+typedef struct {
+  uint64_t num_pis, num_pos, num_gates, num_wires;
+  uint64_t num_elements;     /* PIs + gates + POs */
+  uint64_t num_levels;       /* entries of num_gates_per_level */
+  uint64_t num_faults;
+  uint64_t num_patterns;
+  uint64_t num_rounds;       /* ceil(patterns / 64) */
+} fsimb_info;
+
+/* Counters and timings of the last run. */
+typedef struct {
+  double ms_total, ms_good, ms_sweep, ms_ffr, ms_h2d, ms_d2h;
+  uint64_t n_tiles;          /* 2048-pattern tiles */
+  uint64_t n_stem_sweeps;    /* FFR roots whose observability is swept */
+  uint64_t n_exact_sweeps;   /* faults simulated by an exact sweep (MUX cones) */
+  uint64_t n_traced_faults;
+  uint64_t n_roots;
+  uint64_t sweep_items;      /* (sweep, subtile) work items executed */
+  uint64_t dense_gate_words; /* gate-word evaluations done by the sweeps */
+  uint64_t sweep_alg_bytes;  /* their algorithmic bytes: 8*(fanin+1) each */
+  uint64_t good_gate_words;  /* gate-word evaluations of the good machine */
+  uint64_t max_live;         /* shared-memory slots per sweep */
+  uint32_t words_per_item, block_threads, blocks, smem_bytes;
+  uint64_t device_bytes;     /* device memory held by the handle */
+  uint64_t kernel_launches;  /* kernels launched by the last run */
+  double ms_compute;         /* device time from results init to the last tile */
+} fsimb_stats;
+
+/* Lifecycle.  fsimb_create fails with FSIMB_ERR_CUDA when `device` is not a
+ * usable CUDA device; there is no CPU fallback.  device = -1 creates a
+ * host-only handle that can load inputs and answer the introspection calls
+ * (format checks without a GPU); fsimb_run on it fails with FSIMB_ERR_CUDA. */
+int fsimb_create(int device, fsimb_handle** out);
+int fsimb_destroy(fsimb_handle* h);
+/* Message of the last failed call on h (h may be NULL for fsimb_create). */
+const char* fsimb_last_error(const fsimb_handle* h);
+
+/* Loading.  Replaces Simulator::read(path, path, path) and
+ * Simulator::read(istream&, istream&, istream&) (fsim/simulation.cpp:12-63).
+ * Pattern rows are taken in file order; the reference stores row r at round
+ * tpg[r] (fsim/simulation.cpp:968-969), which is the same whenever
+ * ceil(P/64) <= nPI and undefined otherwise. */
+int fsimb_load_files(fsimb_handle* h, const char* ckt_path, const char* flst_path,
+                     const char* ptn_path);
+int fsimb_load_buffers(fsimb_handle* h, const char* ckt, size_t ckt_len, const char* flst,
+                       size_t flst_len, const char* ptn, size_t ptn_len);
+/* Circuit only (clears faults and patterns). */
+int fsimb_load_circuit(fsimb_handle* h, const char* ckt, size_t ckt_len);
+/* Faults by topological index: pin 0 = output, k = k-th input; value 0/1.
+ * Replaces _read_fault (fsim/simulation.cpp:943-959) for callers that hold
+ * the list in memory; input-pin faults have no reference representation. */
+int fsimb_set_faults(fsimb_handle* h, const uint32_t* site, const uint8_t* pin,
+                     const uint8_t* value, uint64_t n);
+int fsimb_set_fault_text(fsimb_handle* h, const char* flst, size_t flst_len);
+/* Pattern words [ceil(P/64)][nPI], round-major (replaces _read_pattern). */
+int fsimb_set_patterns(fsimb_handle* h, const uint64_t* words, uint64_t num_patterns);
+
+/* Simulation.  Replaces Simulator::run(Mode, threads) (fsim/simulation.cpp:65-92)
+ * and CUDAMAPartitioner::prepare_gpu_simulation()/run() (cuda_MA_partition.cu:496-538).
+ * opts may be NULL.  The call returns after the results are on the host. */
+int fsimb_run(fsimb_handle* h, const fsimb_opts* opts);
+
+/* Results of the last run. */
+int fsimb_results(const fsimb_handle* h, fsimb_fault_result* out, uint64_t n);
+/* The reference's found_fault_to_pattern() view, 2 entries per fault
+ * (fsim/simulation.hpp:89-91). */
+int fsimb_found_fault_to_pattern(const fsimb_handle* h, uint64_t* out, uint64_t n);
+/* Good-machine words of all N elements for one round, masked to the round's
+ * valid bits; topological order [PIs, gates, POs].  After fsimb_run this is
+ * g_pi/g_gate/g_po_results() of the reference for round = num_rounds-1
+ * (fsim/simulation.hpp:57-59). */
+int fsimb_good_values(const fsimb_handle* h, uint64_t round, uint64_t* out, uint64_t n);
+
+/* Introspection (fsim/simulation.hpp:62-94). */
+int fsimb_get_info(const fsimb_handle* h, fsimb_info* out);
+int fsimb_get_stats(const fsimb_handle* h, fsimb_stats* out);
+/* gate_idx_to_tpg_order_idx(): file id -> topological index, n = elements */
+int fsimb_topo_map(const fsimb_handle* h, uint64_t* out, uint64_t n);
+/* level of each element in topological order, n = elements */
+int fsimb_levels(const fsimb_handle* h, uint64_t* out, uint64_t n);
+/* num_gates_per_level(), n = num_levels */
+int fsimb_gates_per_level(const fsimb_handle* h, uint64_t* out, uint64_t n);
+/* gate types in topological order (GateType numbering; PI = 9, PO = 10) */
+int fsimb_types(const fsimb_handle* h, uint8_t* out, uint64_t n);
+/* loaded faults: topological site, pin, value */
+int fsimb_faults(const fsimb_handle* h, uint32_t* site, uint8_t* pin, uint8_t* value, uint64_t n);
+/* loaded pattern words, n = rounds * nPI */
+int fsimb_patterns(const fsimb_handle* h, uint64_t* out, uint64_t n);
+
+/* Synthetic workloads (seeded; text in LSIM's formats).  Returned buffers
+ * are released with fsimb_free_text. */
+typedef struct {
+  uint32_t struct_size;
+  uint64_t seed;
+  uint32_t n_gates, n_pi, n_po, n_levels;
+  uint32_t window;          /* inputs at most this many levels back (4) */
+  double p_fanin3;          /* multi-input gates: P(3 inputs) */
+  uint32_t type_mask;       /* bit t allows GateType t */
+  double hub_frac;          /* fraction of gates with a large fanout target */
+  uint32_t hub_fo_min, hub_fo_max, fo_min, fo_max;
+  double p_unused;
+  int32_t shuffle_ids;
+} fsimb_gen_config;
+int fsimb_gen_circuit(const fsimb_gen_config* cfg, char** text, size_t* len);
+/* Fault list for a circuit given as .ckt text.  kind 0: every gate output
+ * SA0/SA1 (plain .flst); 1: outputs and input pins; 2: outputs and input pins
+ * collapsed by equivalence (pin lists use the "@pins" .flst form). */
+int fsimb_gen_faults(const char* ckt, size_t ckt_len, int kind, char** text, size_t* len);
+int fsimb_gen_patterns(uint64_t seed, uint64_t n_patterns, uint64_t n_pi, double biased_pi_frac,
+                       double p_one_biased, char** text, size_t* len);
+void fsimb_free_text(char* text);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FSIMB_H */

@@ -1,0 +1,140 @@
+"""ctypes binding of the C ABI in include/fsimb.h.
+
+The shared library ``lsim_b200/libfsimb200.so`` is built in-tree from
+``lsim_b200/csrc`` (``python -m lsim_b200.build``).  If it is missing it is
+built on first use; if that fails the import fails -- there is no CPU
+fallback for the simulation path.
+"""
+import ctypes
+import os
+
+from . import build as _build
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+OK, ERR_ARG, ERR_PARSE, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_IO, ERR_LIMIT = range(8)
+_ERR_NAMES = {1: "ARG", 2: "PARSE", 3: "CUDA", 4: "STATE", 5: "NOMEM", 6: "IO", 7: "LIMIT"}
+
+
+class FsimbError(RuntimeError):
+    """A failed C-ABI call: ``code`` is the FSIMB_ERR_* status."""
+
+    def __init__(self, code, msg):
+        super().__init__("FSIMB_ERR_%s: %s" % (_ERR_NAMES.get(code, str(code)), msg))
+        self.code = code
+
+
+class FaultResult(ctypes.Structure):
+    _fields_ = [("detected", ctypes.c_uint8), ("ref_last_round_flag", ctypes.c_uint8),
+                ("pad", ctypes.c_uint8 * 6), ("first_pattern", ctypes.c_int64),
+                ("count", ctypes.c_uint64), ("ref_last_rd", ctypes.c_uint64)]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("drop", ctypes.c_uint32),
+                ("words_per_item", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("stream", ctypes.c_void_p)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ["num_pis", "num_pos", "num_gates", "num_wires", "num_elements", "num_levels",
+                 "num_faults", "num_patterns", "num_rounds"]]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in
+                 ["ms_total", "ms_good", "ms_sweep", "ms_ffr", "ms_h2d", "ms_d2h"]] +
+                [(n, ctypes.c_uint64) for n in
+                 ["n_tiles", "n_stem_sweeps", "n_exact_sweeps", "n_traced_faults", "n_roots",
+                  "sweep_items", "dense_gate_words", "sweep_alg_bytes", "good_gate_words",
+                  "max_live"]] +
+                [(n, ctypes.c_uint32) for n in
+                 ["words_per_item", "block_threads", "blocks", "smem_bytes"]] +
+                [("device_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                 ("ms_compute", ctypes.c_double)])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class GenConfig(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("seed", ctypes.c_uint64),
+                ("n_gates", ctypes.c_uint32), ("n_pi", ctypes.c_uint32),
+                ("n_po", ctypes.c_uint32), ("n_levels", ctypes.c_uint32),
+                ("window", ctypes.c_uint32), ("p_fanin3", ctypes.c_double),
+                ("type_mask", ctypes.c_uint32), ("hub_frac", ctypes.c_double),
+                ("hub_fo_min", ctypes.c_uint32), ("hub_fo_max", ctypes.c_uint32),
+                ("fo_min", ctypes.c_uint32), ("fo_max", ctypes.c_uint32),
+                ("p_unused", ctypes.c_double), ("shuffle_ids", ctypes.c_int32)]
+
+
+# Every symbol the header declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_U32P = ctypes.POINTER(ctypes.c_uint32)
+_U8P = ctypes.POINTER(ctypes.c_uint8)
+_CP = ctypes.c_char_p
+_SZ = ctypes.c_size_t
+SIGNATURES = {
+    "fsimb_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "fsimb_destroy": (ctypes.c_int, [_P]),
+    "fsimb_last_error": (_CP, [_P]),
+    "fsimb_load_files": (ctypes.c_int, [_P, _CP, _CP, _CP]),
+    "fsimb_load_buffers": (ctypes.c_int, [_P, _CP, _SZ, _CP, _SZ, _CP, _SZ]),
+    "fsimb_load_circuit": (ctypes.c_int, [_P, _CP, _SZ]),
+    "fsimb_set_faults": (ctypes.c_int, [_P, _U32P, _U8P, _U8P, _U64]),
+    "fsimb_set_fault_text": (ctypes.c_int, [_P, _CP, _SZ]),
+    "fsimb_set_patterns": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_run": (ctypes.c_int, [_P, ctypes.POINTER(Opts)]),
+    "fsimb_results": (ctypes.c_int, [_P, ctypes.POINTER(FaultResult), _U64]),
+    "fsimb_found_fault_to_pattern": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_good_values": (ctypes.c_int, [_P, _U64, _U64P, _U64]),
+    "fsimb_get_info": (ctypes.c_int, [_P, ctypes.POINTER(Info)]),
+    "fsimb_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
+    "fsimb_topo_map": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_levels": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_gates_per_level": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_types": (ctypes.c_int, [_P, _U8P, _U64]),
+    "fsimb_faults": (ctypes.c_int, [_P, _U32P, _U8P, _U8P, _U64]),
+    "fsimb_patterns": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_gen_circuit": (ctypes.c_int, [ctypes.POINTER(GenConfig), ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(_SZ)]),
+    "fsimb_gen_faults": (ctypes.c_int, [_CP, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(_SZ)]),
+    "fsimb_gen_patterns": (ctypes.c_int, [_U64, _U64, _U64, ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ)]),
+    "fsimb_free_text": (None, [ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads (building first if needed) the in-tree library."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            _build.build()
+        L = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code, handle=None):
+    if code != OK:
+        msg = lib().fsimb_last_error(handle)
+        raise FsimbError(code, msg.decode() if msg else "")
+
+
+def take_text(ptr, n):
+    try:
+        return ctypes.string_at(ptr, n.value).decode()
+    finally:
+        lib().fsimb_free_text(ptr)

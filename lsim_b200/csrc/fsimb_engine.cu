@@ -1,0 +1,914 @@
+// Handle, device memory and run orchestration behind the C ABI (include/fsimb.h).
+//
+// One run:
+//   1. upload the compiled plan (once per circuit + fault list) and patterns;
+//   2. good machine for all words, level by level (k_good_level);
+//   3. per 2048-pattern tile: stem / exact sweeps (k_sweep<M>), FFR tracing
+//      and per-fault accumulation (k_ffr, k_exact), and in drop mode the
+//      compaction of what is still undetected (k_drop);
+//   4. per-fault counters back to the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/fsimb.h"
+#include "fsimb_gen.h"
+#include "fsimb_kernels.cuh"
+#include "fsimb_netlist.h"
+#include "fsimb_plan.h"
+
+using namespace fsimb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError {
+  std::string msg;
+};
+struct LimitError {
+  std::string msg;
+};
+struct StateError {
+  std::string msg;
+};
+struct ArgError {
+  std::string msg;
+};
+struct IoError {
+  std::string msg;
+};
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_)};                \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  void ensure(size_t bytes) {
+    if (bytes <= n && p) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      throw CudaError{"cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
+    }
+    n = bytes;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
+  b.ensure(v.size() * sizeof(T));
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+std::string read_file(const char* path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw IoError{std::string("cannot open ") + path};
+  std::ostringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+}  // namespace
+
+struct fsimb_handle {
+  int device = -1;
+  int n_sms = 0;
+  size_t smem_optin = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  Netlist nl;
+  bool has_ckt = false;
+  std::vector<Fault> faults;
+  bool has_faults = false;
+  Patterns pats;
+  bool has_pats = false;
+
+  Plan plan;
+  bool plan_valid = false;
+  bool plan_uploaded = false;
+
+  DevBuf d_type, d_fi_off, d_fi_idx, d_fslot, d_meta, d_level, d_level_off, d_li_off, d_li_elem;
+  DevBuf d_roots, d_members, d_traced, d_inj, d_exact;
+  DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue;
+  DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout;
+  uint64_t good_tiles = 0;  // tiles held in d_good
+  uint64_t good_P = 0;
+  bool pats_uploaded = false;  // d_pwords holds the current patterns
+
+  std::vector<fsimb_fault_result> results;
+  bool has_results = false;
+  fsimb_stats stats{};
+  std::vector<cudaEvent_t> events;
+
+  ~fsimb_handle() {
+    if (device >= 0) {
+      cudaSetDevice(device);
+      for (DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_fslot, &d_meta, &d_level, &d_level_off,
+                        &d_li_off, &d_li_elem, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+                        &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
+                        &d_queue, &d_root_list[0], &d_root_list[1], &d_sweep_list,
+                        &d_exact_list[0], &d_exact_list[1], &d_nout})
+        b->release();
+      for (auto e : events) cudaEventDestroy(e);
+      if (stream) cudaStreamDestroy(stream);
+    }
+  }
+
+  cudaEvent_t ev(size_t i) {
+    while (events.size() <= i) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      events.push_back(e);
+    }
+    return events[i];
+  }
+
+  uint64_t device_bytes() const {
+    uint64_t s = 0;
+    for (const DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_fslot, &d_meta, &d_level, &d_level_off,
+                            &d_li_off, &d_li_elem, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+                            &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
+                            &d_queue, &d_root_list[0], &d_root_list[1], &d_sweep_list,
+                            &d_exact_list[0], &d_exact_list[1], &d_nout})
+      s += b->n;
+    return s;
+  }
+
+  void invalidate_circuit() {
+    has_faults = false;
+    has_pats = false;
+    plan_valid = false;
+    plan_uploaded = false;
+    has_results = false;
+    good_tiles = 0;
+  }
+
+  void load_ckt(const char* t, size_t n) {
+    Netlist tmp;
+    parse_ckt(t, n, tmp);
+    nl = std::move(tmp);
+    has_ckt = true;
+    invalidate_circuit();
+    faults.clear();
+    pats = Patterns();
+  }
+  void load_flst(const char* t, size_t n) {
+    if (!has_ckt) throw StateError{"load a circuit first"};
+    std::vector<Fault> tmp;
+    parse_flst(t, n, nl, tmp);
+    faults = std::move(tmp);
+    has_faults = true;
+    plan_valid = false;
+    plan_uploaded = false;
+    has_results = false;
+  }
+  void load_ptn(const char* t, size_t n) {
+    if (!has_ckt) throw StateError{"load a circuit first"};
+    Patterns tmp;
+    parse_ptn(t, n, nl, tmp);
+    pats = std::move(tmp);
+    has_pats = true;
+    has_results = false;
+    good_tiles = 0;
+    pats_uploaded = false;
+  }
+
+  void run(const fsimb_opts* opts);
+};
+
+// --------------------------------------------------------------------------
+void fsimb_handle::run(const fsimb_opts* opts) {
+  if (device < 0) throw CudaError{"host-only handle: no GPU to run on"};
+  if (!has_ckt || !has_faults || !has_pats) throw StateError{"load circuit, faults and patterns first"};
+  fsimb_opts o{};
+  if (opts) {
+    if (opts->struct_size != 0 && opts->struct_size < sizeof(fsimb_opts))
+      throw ArgError{"fsimb_opts.struct_size too small"};
+    o = *opts;
+  }
+  if (o.words_per_item && o.words_per_item != 1 && o.words_per_item != 2 && o.words_per_item != 4 &&
+      o.words_per_item != 8)
+    throw ArgError{"words_per_item must be 0, 1, 2, 4 or 8"};
+  if (o.block_threads && (o.block_threads < 32 || o.block_threads > 512 || o.block_threads % 32))
+    throw ArgError{"block_threads must be 0 or a multiple of 32 in 32..512"};
+  CK(cudaSetDevice(device));
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : stream;
+  has_results = false;
+
+  if (!plan_valid) {
+    build_plan(nl, faults, plan);
+    plan_valid = true;
+    plan_uploaded = false;
+  }
+  const uint32_t N = plan.N;
+  const uint64_t F = faults.size();
+  const uint64_t W = pats.W;
+  const uint64_t tiles = (W + kTileWords - 1) / kTileWords;
+  const uint64_t W_pad = tiles * kTileWords;
+  const uint32_t n_sweeps = (uint32_t)plan.sweeps.size();
+  const uint32_t n_roots = (uint32_t)plan.roots.size();
+  const uint32_t n_exact = (uint32_t)plan.exact_fault.size();
+  if (W_pad > (1ull << 31) || tiles * (uint64_t)N * kTileWords > (1ull << 40))
+    throw LimitError{"pattern block too large"};
+
+  // Sweep shape: M words per item, CTA size, CTAs per SM.
+  const size_t static_smem = 256;
+  const size_t budget = smem_optin > static_smem + 1024 ? smem_optin - static_smem - 1024 : 0;
+  int M = (int)o.words_per_item;
+  if (!M) {
+    M = 8;
+    while (M > 1 && (size_t)plan.max_live * M * 8 > budget) M /= 2;
+    // keep at least ~4 items per SM in flight for narrow circuits
+  }
+  const size_t smem = std::max<size_t>(16, (size_t)plan.max_live * M * 8);
+  if (smem > budget)
+    throw LimitError{"a sweep needs " + std::to_string(plan.max_live) +
+                     " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
+                     " at " + std::to_string(M) + " word(s) per item"};
+  int threads = (int)o.block_threads;
+  if (!threads) {
+    uint32_t w = std::max<uint32_t>(plan.max_level_width, 1);
+    threads = (int)std::min<uint32_t>(512, std::max<uint32_t>(64, (w + 31) / 32 * 32));
+  }
+
+  cudaEvent_t e0 = ev(0), e1 = ev(1), e2 = ev(2), e3 = ev(3);
+  CK(cudaEventRecord(e0, s));
+  if (!plan_uploaded) {
+    upload(d_type, nl.type, s);
+    upload(d_fi_off, nl.fi_off, s);
+    upload(d_fi_idx, nl.fi_idx, s);
+    upload(d_fslot, plan.fslot, s);
+    upload(d_meta, plan.meta, s);
+    upload(d_level, nl.level, s);
+    upload(d_level_off, plan.level_off, s);
+    upload(d_li_off, plan.li_off, s);
+    upload(d_li_elem, plan.li_elem, s);
+    upload(d_roots, plan.roots, s);
+    upload(d_members, plan.members, s);
+    upload(d_traced, plan.traced, s);
+    upload(d_inj, plan.sweeps, s);
+    upload(d_exact, plan.exact_fault, s);
+    plan_uploaded = true;
+  }
+  if (!pats_uploaded) {
+    upload(d_pwords, pats.words, s);
+    pats_uploaded = true;
+  }
+  uint64_t launches = 1;  // results init
+  d_good.ensure(tiles * N * kTileWords * 8);
+  d_sens.ensure((size_t)N * kTileWords * 8);
+  d_out.ensure((size_t)std::max<uint32_t>(n_sweeps, 1) * kTileWords * 8);
+  d_count.ensure(std::max<uint64_t>(F, 1) * 8);
+  d_first.ensure(std::max<uint64_t>(F, 1) * 8);
+  d_lastflag.ensure(std::max<uint64_t>(F, 1));
+  d_queue.ensure(std::max<uint64_t>(tiles, 1) * sizeof(int));
+  if (o.drop) {
+    d_root_list[0].ensure(std::max<uint32_t>(n_roots, 1) * 4);
+    d_root_list[1].ensure(std::max<uint32_t>(n_roots, 1) * 4);
+    d_sweep_list.ensure(std::max<uint32_t>(n_sweeps, 1) * 4);
+    d_exact_list[0].ensure(std::max<uint32_t>(n_exact, 1) * 4);
+    d_exact_list[1].ensure(std::max<uint32_t>(n_exact, 1) * 4);
+    d_nout.ensure(16);
+  }
+  CK(cudaMemsetAsync(d_queue.p, 0, std::max<uint64_t>(tiles, 1) * sizeof(int), s));
+  launch_init_results(d_count.as<unsigned long long>(), d_first.as<unsigned long long>(),
+                      d_lastflag.as<uint8_t>(), (uint32_t)F, s);
+  CK(cudaEventRecord(e1, s));
+
+  // 2. good machine
+  for (uint32_t l = 0; l < nl.n_levels; ++l) {
+    GoodArgs g{};
+    g.type = d_type.as<uint8_t>();
+    g.fi_off = d_fi_off.as<uint32_t>();
+    g.fi_idx = d_fi_idx.as<uint32_t>();
+    g.pwords = d_pwords.as<uint64_t>();
+    g.good = d_good.as<uint64_t>();
+    g.n_pi = (uint32_t)nl.n_pi;
+    g.N = N;
+    g.lo = nl.level_off[l];
+    g.hi = nl.level_off[l + 1];
+    g.W = (uint32_t)W;
+    g.W_pad = (uint32_t)W_pad;
+    launch_good_level(g, s);
+    launches += (g.hi > g.lo) ? 1 : 0;
+  }
+  CK(cudaGetLastError());
+  good_tiles = tiles;
+  good_P = pats.P;
+  CK(cudaEventRecord(e2, s));
+
+  CK(sweep_set_smem(M, smem));
+  int occ = 0;
+  CK(sweep_occupancy(M, threads, smem, &occ));
+  if (occ < 1) throw LimitError{"sweep kernel does not fit on an SM with this shape"};
+  const int blocks = n_sms * occ;
+
+  // 3. tiles
+  uint32_t n_sw = n_sweeps, n_rt = n_roots, n_ex = n_exact;
+  const uint32_t* sw_list = nullptr;
+  const uint32_t* rt_list = nullptr;
+  const uint32_t* ex_list = nullptr;
+  int cur = 0;
+  uint64_t items = 0, dense = 0, alg_bytes = 0;
+  float ms_sweep = 0, ms_ffr = 0;
+  const uint32_t gates_end = plan.level_off[std::min(plan.max_gate_level + 1, plan.n_levels)];
+  std::vector<uint32_t> host_sw;  // only for the dense-work counter in drop mode
+  for (uint64_t t = 0; t < tiles; ++t) {
+    const uint64_t* good_t = d_good.as<uint64_t>() + t * (uint64_t)N * kTileWords;
+    cudaEvent_t a0 = ev(4 + 3 * t), a1 = ev(5 + 3 * t), a2 = ev(6 + 3 * t);
+    CK(cudaEventRecord(a0, s));
+    if (n_sw) {
+      SweepArgs sa{};
+      sa.fslot = d_fslot.as<uint4>();
+      sa.meta = d_meta.as<uint32_t>();
+      sa.level = d_level.as<uint32_t>();
+      sa.level_off = d_level_off.as<uint32_t>();
+      sa.li_off = d_li_off.as<uint32_t>();
+      sa.li_elem = d_li_elem.as<uint32_t>();
+      sa.fi_off = d_fi_off.as<uint32_t>();
+      sa.fi_idx = d_fi_idx.as<uint32_t>();
+      sa.type = d_type.as<uint8_t>();
+      sa.inj = d_inj.as<InjRec>();
+      sa.list = sw_list;
+      sa.n_list = n_sw;
+      sa.subtiles = kTileWords / M;
+      sa.max_gate_level = plan.max_gate_level;
+      sa.N = N;
+      sa.good = good_t;
+      sa.out = d_out.as<uint64_t>();
+      sa.queue = d_queue.as<int>() + t;
+      const int nb = (int)std::min<uint64_t>((uint64_t)blocks, (uint64_t)n_sw * sa.subtiles);
+      CK(launch_sweep(M, threads, nb, smem, sa, s));
+      ++launches;
+      items += (uint64_t)n_sw * sa.subtiles;
+      if (!sw_list) {
+        dense += plan.dense_sweep_gates * kTileWords;
+        alg_bytes += plan.dense_sweep_bytes * kTileWords;
+      } else {
+        host_sw.resize(n_sw);
+        CK(cudaMemcpyAsync(host_sw.data(), sw_list, n_sw * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (uint32_t si : host_sw) {
+          uint32_t L0 = nl.level[plan.sweeps[si].elem] + 1;
+          if (L0 <= plan.max_gate_level) {
+            dense += (uint64_t)(gates_end - plan.level_off[L0]) * kTileWords;
+            alg_bytes += (plan.nfp_prefix[gates_end] - plan.nfp_prefix[plan.level_off[L0]]) * kTileWords;
+          }
+        }
+      }
+    }
+    CK(cudaEventRecord(a1, s));
+    FfrArgs fa{};
+    fa.roots = d_roots.as<RootRec>();
+    fa.list = rt_list;
+    fa.n_list = n_rt;
+    fa.members = d_members.as<MemberRec>();
+    fa.traced = d_traced.as<TracedRec>();
+    fa.fi_off = d_fi_off.as<uint32_t>();
+    fa.fi_idx = d_fi_idx.as<uint32_t>();
+    fa.type = d_type.as<uint8_t>();
+    fa.good = good_t;
+    fa.obs = d_out.as<uint64_t>();
+    fa.sens = d_sens.as<uint64_t>();
+    fa.tile = (uint32_t)t;
+    fa.W = (uint32_t)W;
+    fa.P = pats.P;
+    fa.drop = o.drop ? 1 : 0;
+    fa.count = d_count.as<unsigned long long>();
+    fa.first = d_first.as<unsigned long long>();
+    fa.lastflag = d_lastflag.as<uint8_t>();
+    launch_ffr(fa, s);
+    launches += n_rt ? 1 : 0;
+    ExactArgs xa{};
+    xa.exact_fault = d_exact.as<uint32_t>();
+    xa.list = ex_list;
+    xa.n_exact = n_ex;
+    xa.first_sweep = plan.n_stem_sweeps;
+    xa.out = d_out.as<uint64_t>();
+    xa.tile = (uint32_t)t;
+    xa.W = (uint32_t)W;
+    xa.P = pats.P;
+    xa.drop = o.drop ? 1 : 0;
+    xa.count = fa.count;
+    xa.first = fa.first;
+    xa.lastflag = fa.lastflag;
+    launch_exact(xa, s);
+    launches += n_ex ? 1 : 0;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(a2, s));
+    if (o.drop && t + 1 < tiles) {
+      CK(cudaMemsetAsync(d_nout.p, 0, 16, s));
+      DropArgs da{};
+      da.roots = d_roots.as<RootRec>();
+      da.in_list = rt_list;
+      da.n_in = n_rt;
+      da.n_in_pad = (n_rt + 31) / 32 * 32;
+      da.traced = d_traced.as<TracedRec>();
+      da.exact_fault = d_exact.as<uint32_t>();
+      da.exact_in = ex_list;
+      da.n_exact_in = n_ex;
+      da.first_exact_sweep = plan.n_stem_sweeps;
+      da.count = d_count.as<unsigned long long>();
+      da.out_roots = d_root_list[cur].as<uint32_t>();
+      da.out_sweeps = d_sweep_list.as<uint32_t>();
+      da.out_exact = d_exact_list[cur].as<uint32_t>();
+      da.n_out = d_nout.as<uint32_t>();
+      launch_drop(da, s);
+      ++launches;
+      CK(cudaGetLastError());
+      uint32_t nout[4] = {0, 0, 0, 0};
+      CK(cudaMemcpyAsync(nout, d_nout.p, 16, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      n_rt = nout[0];
+      n_sw = nout[1];
+      n_ex = nout[2];
+      rt_list = d_root_list[cur].as<uint32_t>();
+      sw_list = d_sweep_list.as<uint32_t>();
+      ex_list = d_exact_list[cur].as<uint32_t>();
+      cur ^= 1;
+      if (n_rt == 0 && n_ex == 0) {
+        CK(cudaEventSynchronize(a2));
+        float x = 0;
+        CK(cudaEventElapsedTime(&x, a0, a1));
+        ms_sweep += x;
+        CK(cudaEventElapsedTime(&x, a1, a2));
+        ms_ffr += x;
+        break;
+      }
+    }
+    if (o.drop) {
+      CK(cudaEventSynchronize(a2));
+      float x = 0;
+      CK(cudaEventElapsedTime(&x, a0, a1));
+      ms_sweep += x;
+      CK(cudaEventElapsedTime(&x, a1, a2));
+      ms_ffr += x;
+    }
+  }
+  CK(cudaEventRecord(e3, s));
+
+  // 4. results
+  std::vector<unsigned long long> cnt(F), fst(F);
+  std::vector<uint8_t> lf(F);
+  cudaEvent_t e4 = ev(4 + 3 * tiles + 1);
+  if (F) {
+    CK(cudaMemcpyAsync(cnt.data(), d_count.p, F * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(fst.data(), d_first.p, F * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(lf.data(), d_lastflag.p, F, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaEventRecord(e4, s));
+  CK(cudaStreamSynchronize(s));
+  if (!o.drop) {
+    for (uint64_t t = 0; t < tiles; ++t) {
+      float x = 0;
+      CK(cudaEventElapsedTime(&x, ev(4 + 3 * t), ev(5 + 3 * t)));
+      ms_sweep += x;
+      CK(cudaEventElapsedTime(&x, ev(5 + 3 * t), ev(6 + 3 * t)));
+      ms_ffr += x;
+    }
+  }
+  results.assign(F, fsimb_fault_result{});
+  const uint64_t last_rd = W ? W - 1 : 0;
+  for (uint64_t f = 0; f < F; ++f) {
+    fsimb_fault_result& r = results[f];
+    r.count = cnt[f];
+    r.detected = cnt[f] > 0;
+    r.first_pattern = (fst[f] == ~0ull) ? -1 : (int64_t)fst[f];
+    r.ref_last_round_flag = W ? lf[f] : 0;
+    r.ref_last_rd = last_rd;
+  }
+  has_results = true;
+
+  float x = 0;
+  stats = fsimb_stats{};
+  CK(cudaEventElapsedTime(&x, e0, e4));
+  stats.ms_total = x;
+  CK(cudaEventElapsedTime(&x, e0, e1));
+  stats.ms_h2d = x;
+  CK(cudaEventElapsedTime(&x, e1, e2));
+  stats.ms_good = x;
+  stats.ms_sweep = ms_sweep;
+  stats.ms_ffr = ms_ffr;
+  CK(cudaEventElapsedTime(&x, e3, e4));
+  stats.ms_d2h = x;
+  stats.n_tiles = tiles;
+  stats.n_stem_sweeps = plan.n_stem_sweeps;
+  stats.n_exact_sweeps = n_exact;
+  stats.n_traced_faults = plan.traced.size();
+  stats.n_roots = n_roots;
+  stats.sweep_items = items;
+  stats.dense_gate_words = dense;
+  stats.sweep_alg_bytes = alg_bytes;
+  stats.kernel_launches = launches;
+  CK(cudaEventElapsedTime(&x, e1, e3));
+  stats.ms_compute = x;
+  stats.good_gate_words = (uint64_t)(N - plan.n_pi) * W_pad;
+  stats.max_live = plan.max_live;
+  stats.words_per_item = (uint32_t)M;
+  stats.block_threads = (uint32_t)threads;
+  stats.blocks = (uint32_t)blocks;
+  stats.smem_bytes = (uint32_t)smem;
+  stats.device_bytes = device_bytes();
+}
+
+// -------------------------------------------------------------------- C ABI
+#define API_BEGIN(h)                                 \
+  if (!(h)) return FSIMB_ERR_ARG;                    \
+  try {
+#define API_END(h)                                   \
+  }                                                  \
+  catch (const ParseError& e) {                      \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_PARSE;                          \
+  }                                                  \
+  catch (const CudaError& e) {                       \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_CUDA;                           \
+  }                                                  \
+  catch (const LimitError& e) {                      \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_LIMIT;                          \
+  }                                                  \
+  catch (const StateError& e) {                      \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_STATE;                          \
+  }                                                  \
+  catch (const ArgError& e) {                        \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_ARG;                            \
+  }                                                  \
+  catch (const IoError& e) {                         \
+    (h)->err = e.msg;                                \
+    return FSIMB_ERR_IO;                             \
+  }                                                  \
+  catch (const std::bad_alloc&) {                    \
+    (h)->err = "host allocation failed";             \
+    return FSIMB_ERR_NOMEM;                          \
+  }                                                  \
+  catch (const std::exception& e) {                  \
+    (h)->err = e.what();                             \
+    return FSIMB_ERR_ARG;                            \
+  }                                                  \
+  (h)->err.clear();                                  \
+  return FSIMB_OK;
+
+extern "C" {
+
+int fsimb_create(int device, fsimb_handle** out) {
+  if (!out) return FSIMB_ERR_ARG;
+  *out = nullptr;
+  fsimb_handle* h = nullptr;
+  try {
+    h = new fsimb_handle();
+    if (device >= 0) {
+      int n = 0;
+      cudaError_t e = cudaGetDeviceCount(&n);
+      if (e != cudaSuccess || device >= n) {
+        g_create_error = std::string("no usable CUDA device ") + std::to_string(device) + ": " +
+                         (e != cudaSuccess ? cudaGetErrorString(e) : "index out of range");
+        cudaGetLastError();
+        delete h;
+        return FSIMB_ERR_CUDA;
+      }
+      int major = 0;
+      CK(cudaSetDevice(device));
+      CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+      if (major < 10) throw CudaError{"device is not sm_100 (Blackwell)"};
+      int sms = 0, optin = 0;
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+      CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+      h->device = device;
+      h->n_sms = sms;
+      h->smem_optin = (size_t)optin;
+      CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    }
+  } catch (const CudaError& e) {
+    g_create_error = e.msg;
+    delete h;
+    return FSIMB_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    g_create_error = "host allocation failed";
+    delete h;
+    return FSIMB_ERR_NOMEM;
+  }
+  *out = h;
+  return FSIMB_OK;
+}
+
+int fsimb_destroy(fsimb_handle* h) {
+  if (!h) return FSIMB_ERR_ARG;
+  delete h;
+  return FSIMB_OK;
+}
+
+const char* fsimb_last_error(const fsimb_handle* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int fsimb_load_files(fsimb_handle* h, const char* ckt, const char* flst, const char* ptn) {
+  API_BEGIN(h)
+  if (!ckt || !flst || !ptn) throw ArgError{"null path"};
+  std::string a = read_file(ckt), b = read_file(flst), c = read_file(ptn);
+  h->load_ckt(a.data(), a.size());
+  h->load_flst(b.data(), b.size());
+  h->load_ptn(c.data(), c.size());
+  API_END(h)
+}
+
+int fsimb_load_buffers(fsimb_handle* h, const char* ckt, size_t ckt_len, const char* flst,
+                       size_t flst_len, const char* ptn, size_t ptn_len) {
+  API_BEGIN(h)
+  if (!ckt || !flst || !ptn) throw ArgError{"null buffer"};
+  h->load_ckt(ckt, ckt_len);
+  h->load_flst(flst, flst_len);
+  h->load_ptn(ptn, ptn_len);
+  API_END(h)
+}
+
+int fsimb_load_circuit(fsimb_handle* h, const char* ckt, size_t ckt_len) {
+  API_BEGIN(h)
+  if (!ckt) throw ArgError{"null buffer"};
+  h->load_ckt(ckt, ckt_len);
+  API_END(h)
+}
+
+int fsimb_set_faults(fsimb_handle* h, const uint32_t* site, const uint8_t* pin,
+                     const uint8_t* value, uint64_t n) {
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"load a circuit first"};
+  if (n && (!site || !value)) throw ArgError{"null fault arrays"};
+  std::vector<Fault> fs(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    if (site[i] >= h->nl.N) throw ArgError{"fault site out of range at " + std::to_string(i)};
+    uint8_t p = pin ? pin[i] : 0;
+    if (p > h->nl.fanin_count(site[i])) throw ArgError{"fault pin out of range at " + std::to_string(i)};
+    fs[i] = Fault{site[i], p, (uint8_t)(value[i] ? 1 : 0)};
+  }
+  h->faults = std::move(fs);
+  h->has_faults = true;
+  h->plan_valid = false;
+  h->plan_uploaded = false;
+  h->has_results = false;
+  API_END(h)
+}
+
+int fsimb_set_fault_text(fsimb_handle* h, const char* flst, size_t flst_len) {
+  API_BEGIN(h)
+  if (!flst) throw ArgError{"null buffer"};
+  h->load_flst(flst, flst_len);
+  API_END(h)
+}
+
+int fsimb_set_patterns(fsimb_handle* h, const uint64_t* words, uint64_t num_patterns) {
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"load a circuit first"};
+  const uint64_t W = (num_patterns + 63) / 64;
+  if (W && !words) throw ArgError{"null pattern words"};
+  if (W * h->nl.n_pi > (1ull << 36)) throw LimitError{"pattern block too large"};
+  Patterns p;
+  p.P = num_patterns;
+  p.W = W;
+  p.words.assign(words, words + W * h->nl.n_pi);
+  h->pats = std::move(p);
+  h->has_pats = true;
+  h->has_results = false;
+  h->good_tiles = 0;
+  h->pats_uploaded = false;
+  API_END(h)
+}
+
+int fsimb_run(fsimb_handle* h, const fsimb_opts* opts) {
+  API_BEGIN(h)
+  h->run(opts);
+  API_END(h)
+}
+
+int fsimb_results(const fsimb_handle* hc, fsimb_fault_result* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_results) throw StateError{"no results: call fsimb_run first"};
+  if (n != h->results.size() || (n && !out)) throw ArgError{"result buffer size must equal the fault count"};
+  std::memcpy(out, h->results.data(), n * sizeof(fsimb_fault_result));
+  API_END(h)
+}
+
+int fsimb_found_fault_to_pattern(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_results) throw StateError{"no results: call fsimb_run first"};
+  if (n != 2 * h->results.size() || (n && !out)) throw ArgError{"buffer size must be 2 * faults"};
+  for (size_t f = 0; f < h->results.size(); ++f) {
+    out[2 * f] = h->results[f].ref_last_round_flag;
+    out[2 * f + 1] = h->results[f].ref_last_rd;
+  }
+  API_END(h)
+}
+
+int fsimb_good_values(const fsimb_handle* hc, uint64_t round, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->good_tiles || h->good_P != h->pats.P) throw StateError{"no good values: call fsimb_run first"};
+  if (round >= h->pats.W) throw ArgError{"round out of range"};
+  if (n != h->nl.N || !out) throw ArgError{"buffer size must equal the element count"};
+  CK(cudaSetDevice(h->device));
+  const uint64_t tile = round / kTileWords, lane = round % kTileWords;
+  const uint64_t* src = h->d_good.as<uint64_t>() + (tile * h->nl.N) * kTileWords + lane;
+  CK(cudaMemcpy2DAsync(out, 8, src, kTileWords * 8, 8, h->nl.N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const uint32_t bits = h->pats.bits(round);
+  const uint64_t mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+  for (uint64_t i = 0; i < n; ++i) out[i] &= mask;
+  API_END(h)
+}
+
+int fsimb_get_info(const fsimb_handle* hc, fsimb_info* out) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!out) throw ArgError{"null output"};
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  *out = fsimb_info{};
+  out->num_pis = h->nl.n_pi;
+  out->num_pos = h->nl.n_po;
+  out->num_gates = h->nl.n_gates;
+  out->num_wires = h->nl.n_wires;
+  out->num_elements = h->nl.N;
+  out->num_levels = h->nl.n_levels;
+  out->num_faults = h->has_faults ? h->faults.size() : 0;
+  out->num_patterns = h->has_pats ? h->pats.P : 0;
+  out->num_rounds = h->has_pats ? h->pats.W : 0;
+  API_END(h)
+}
+
+int fsimb_get_stats(const fsimb_handle* hc, fsimb_stats* out) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!out) throw ArgError{"null output"};
+  *out = h->stats;
+  API_END(h)
+}
+
+int fsimb_topo_map(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  if (n != h->nl.N || !out) throw ArgError{"buffer size must equal the element count"};
+  std::copy(h->nl.tpg.begin(), h->nl.tpg.end(), out);
+  API_END(h)
+}
+
+int fsimb_levels(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  if (n != h->nl.N || !out) throw ArgError{"buffer size must equal the element count"};
+  for (uint64_t i = 0; i < n; ++i) out[i] = h->nl.level[i];
+  API_END(h)
+}
+
+int fsimb_gates_per_level(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  if (n != h->nl.n_levels || !out) throw ArgError{"buffer size must equal the level count"};
+  std::copy(h->nl.per_level.begin(), h->nl.per_level.end(), out);
+  API_END(h)
+}
+
+int fsimb_types(const fsimb_handle* hc, uint8_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  if (n != h->nl.N || !out) throw ArgError{"buffer size must equal the element count"};
+  std::copy(h->nl.type.begin(), h->nl.type.end(), out);
+  API_END(h)
+}
+
+int fsimb_faults(const fsimb_handle* hc, uint32_t* site, uint8_t* pin, uint8_t* value, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_faults) throw StateError{"no faults loaded"};
+  if (n != h->faults.size()) throw ArgError{"buffer size must equal the fault count"};
+  for (uint64_t i = 0; i < n; ++i) {
+    if (site) site[i] = h->faults[i].site;
+    if (pin) pin[i] = h->faults[i].pin;
+    if (value) value[i] = h->faults[i].value;
+  }
+  API_END(h)
+}
+
+int fsimb_patterns(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!h->has_pats) throw StateError{"no patterns loaded"};
+  if (n != h->pats.words.size() || (n && !out)) throw ArgError{"buffer size must equal rounds * PIs"};
+  std::copy(h->pats.words.begin(), h->pats.words.end(), out);
+  API_END(h)
+}
+
+static int emit_text(const std::string& s, char** text, size_t* len) {
+  char* p = (char*)std::malloc(s.size() + 1);
+  if (!p) return FSIMB_ERR_NOMEM;
+  std::memcpy(p, s.data(), s.size());
+  p[s.size()] = 0;
+  *text = p;
+  if (len) *len = s.size();
+  return FSIMB_OK;
+}
+
+int fsimb_gen_circuit(const fsimb_gen_config* cfg, char** text, size_t* len) {
+  if (!cfg || !text) return FSIMB_ERR_ARG;
+  try {
+    GenConfig g;
+    g.seed = cfg->seed;
+    g.n_gates = cfg->n_gates;
+    g.n_pi = cfg->n_pi;
+    g.n_po = cfg->n_po;
+    g.n_levels = cfg->n_levels;
+    if (cfg->window) g.window = cfg->window;
+    g.p_fanin3 = cfg->p_fanin3;
+    if (cfg->type_mask) g.type_mask = cfg->type_mask;
+    g.hub_frac = cfg->hub_frac;
+    if (cfg->hub_fo_min) g.hub_fo_min = cfg->hub_fo_min;
+    if (cfg->hub_fo_max) g.hub_fo_max = cfg->hub_fo_max;
+    if (cfg->fo_min) g.fo_min = cfg->fo_min;
+    if (cfg->fo_max) g.fo_max = cfg->fo_max;
+    g.p_unused = cfg->p_unused;
+    g.shuffle_ids = cfg->shuffle_ids;
+    if (g.n_pi == 0 || g.n_levels == 0) {
+      g_create_error = "generator needs at least one PI and one level";
+      return FSIMB_ERR_ARG;
+    }
+    if (g.hub_fo_max < g.hub_fo_min || g.fo_max < g.fo_min) {
+      g_create_error = "generator fanout range is empty";
+      return FSIMB_ERR_ARG;
+    }
+    return emit_text(generate_ckt(g), text, len);
+  } catch (const std::bad_alloc&) {
+    return FSIMB_ERR_NOMEM;
+  }
+}
+
+int fsimb_gen_faults(const char* ckt, size_t ckt_len, int kind, char** text, size_t* len) {
+  if (!ckt || !text || kind < 0 || kind > 2) return FSIMB_ERR_ARG;
+  try {
+    Netlist nl;
+    parse_ckt(ckt, ckt_len, nl);
+    std::vector<Fault> fs;
+    build_fault_list(nl, (FaultListKind)kind, fs);
+    return emit_text(write_flst(nl, fs, kind != 0), text, len);
+  } catch (const ParseError& e) {
+    g_create_error = e.msg;
+    return FSIMB_ERR_PARSE;
+  } catch (const std::bad_alloc&) {
+    return FSIMB_ERR_NOMEM;
+  }
+}
+
+int fsimb_gen_patterns(uint64_t seed, uint64_t n_patterns, uint64_t n_pi, double biased_pi_frac,
+                       double p_one_biased, char** text, size_t* len) {
+  if (!text || n_pi == 0) return FSIMB_ERR_ARG;
+  try {
+    PatternConfig pc;
+    pc.seed = seed;
+    pc.n_patterns = n_patterns;
+    pc.biased_pi_frac = biased_pi_frac;
+    pc.p_one_biased = p_one_biased;
+    Patterns p;
+    generate_patterns(pc, n_pi, p);
+    return emit_text(write_ptn(p, n_pi), text, len);
+  } catch (const std::bad_alloc&) {
+    return FSIMB_ERR_NOMEM;
+  }
+}
+
+void fsimb_free_text(char* text) { std::free(text); }
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// Device kernels of the B200 stuck-at fault simulator.  All arithmetic is
+// bitwise on 64-bit words (64 patterns per word); no tensor cores are
+// involved because gate evaluation is not a contraction.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fsimb_plan.h"
+
+namespace fsimb {
+
+struct GoodArgs {
+  const uint8_t* type;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint64_t* pwords;  // [W][n_pi]
+  uint64_t* good;          // [tiles][N][32]
+  uint32_t n_pi, N;
+  uint32_t lo, hi;         // element range of one level
+  uint32_t W, W_pad;       // real and padded word counts
+};
+
+struct SweepArgs {
+  const uint4* fslot;
+  const uint32_t* meta;
+  const uint32_t* level;
+  const uint32_t* level_off;
+  const uint32_t* li_off;
+  const uint32_t* li_elem;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const InjRec* inj;
+  const uint32_t* list;    // sweep indices to run (nullptr: 0..n_list-1)
+  uint32_t n_list;
+  uint32_t subtiles;       // 32 / M
+  uint32_t max_gate_level;
+  uint32_t N;
+  const uint64_t* good;    // this tile: [N][32]
+  uint64_t* out;           // this tile: [n_sweeps][32] OR of PO differences
+  int* queue;              // work counter for this launch
+};
+
+struct FfrArgs {
+  const RootRec* roots;
+  const uint32_t* list;    // root indices to process (nullptr: all)
+  uint32_t n_list;
+  const MemberRec* members;
+  const TracedRec* traced;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const uint64_t* good;    // tile [N][32]
+  const uint64_t* obs;     // tile [n_sweeps][32]
+  uint64_t* sens;          // scratch [N][32]
+  uint32_t tile, W;
+  uint64_t P;
+  int drop;                // skip faults detected in an earlier tile
+  unsigned long long* count;
+  unsigned long long* first;
+  uint8_t* lastflag;
+};
+
+struct ExactArgs {
+  const uint32_t* exact_fault;
+  const uint32_t* list;    // exact indices to process (nullptr: all)
+  uint32_t n_exact;
+  uint32_t first_sweep;    // index of the first exact sweep
+  const uint64_t* out;     // tile [n_sweeps][32]
+  uint32_t tile, W;
+  uint64_t P;
+  int drop;
+  unsigned long long* count;
+  unsigned long long* first;
+  uint8_t* lastflag;
+};
+
+// Threads [0, n_in_pad) handle roots, the rest exact faults.
+struct DropArgs {
+  const RootRec* roots;
+  const uint32_t* in_list;   // current live roots (nullptr: all)
+  uint32_t n_in, n_in_pad;
+  const TracedRec* traced;
+  const uint32_t* exact_fault;
+  const uint32_t* exact_in;  // current live exact indices (nullptr: all)
+  uint32_t n_exact_in;
+  uint32_t first_exact_sweep;
+  const unsigned long long* count;
+  uint32_t* out_roots;       // surviving root indices
+  uint32_t* out_sweeps;      // sweeps still needed (stem flips and exact faults)
+  uint32_t* out_exact;       // surviving exact indices
+  uint32_t* n_out;           // [3]: roots, sweeps, exact
+};
+
+void launch_good_level(const GoodArgs& a, cudaStream_t s);
+// Returns cudaErrorInvalidValue when M is unsupported.
+cudaError_t launch_sweep(int M, int threads, int blocks, size_t smem, const SweepArgs& a,
+                         cudaStream_t s);
+cudaError_t sweep_set_smem(int M, size_t smem);
+cudaError_t sweep_occupancy(int M, int threads, size_t smem, int* blocks_per_sm);
+void launch_ffr(const FfrArgs& a, cudaStream_t s);
+void launch_exact(const ExactArgs& a, cudaStream_t s);
+void launch_init_results(unsigned long long* count, unsigned long long* first, uint8_t* lastflag,
+                         uint32_t F, cudaStream_t s);
+void launch_drop(const DropArgs& a, cudaStream_t s);
+
+}  // namespace fsimb

@@ -1,0 +1,81 @@
+"""Seeded synthetic workloads in LSIM's .ckt / .flst / .ptn formats.
+
+The generator (lsim_b200/csrc/fsimb_gen.cpp) builds levelized combinational
+DAGs: gates spread evenly over the levels, types drawn uniformly from the
+allowed set, fan-in 2-3 (1 for NOT/BUF, 3 for MUX), inputs from at most
+``window`` levels back with preferential attachment, the first input always
+from the previous level; POs are driven by sink gates of the top levels.
+
+``WORKLOADS`` holds the benchmark configurations:
+  c1  2,000 gates, 64 PI / 64 PO, 30 levels, SA0/SA1 on every gate output
+      (4,000 faults), 4,096 uniform patterns (seed 0);
+  c2  200,000 gates, 1,000 PI / 1,000 PO, 150 levels, mean fan-in 2.2,
+      SA0/SA1 on every gate output and input pin collapsed by equivalence,
+      65,536 uniform patterns;
+  c3  2,000,000 gates, 5,000 PI / 5,000 PO, 400 levels, 10% of gates with a
+      fanout target of 8-64 (the rest 1-3), output + input-pin faults
+      collapsed, 16,384 patterns with half of the PIs at P(1) = 0.2.
+"""
+import ctypes
+
+from . import _lib
+
+# GateType numbering (fsim/base_ppg.hpp:19-32)
+INV, AND, OR, XOR, NAND, NOR, XNOR, MUX, CLKBUF = range(9)
+BENCH_TYPES = (1 << AND) | (1 << OR) | (1 << NAND) | (1 << NOR) | (1 << XOR) | (1 << XNOR) | \
+    (1 << INV) | (1 << CLKBUF)
+ALL_TYPES = BENCH_TYPES | (1 << MUX)
+FAULT_KINDS = {"outputs": 0, "pins": 1, "collapsed": 2}
+
+WORKLOADS = {
+    "c1": dict(n_gates=2000, n_pi=64, n_po=64, n_levels=30, p_fanin3=0.5, seed=0,
+               n_patterns=4096, faults="outputs"),
+    "c2": dict(n_gates=200000, n_pi=1000, n_po=1000, n_levels=150, p_fanin3=0.6, seed=0,
+               n_patterns=65536, faults="collapsed"),
+    "c3": dict(n_gates=2000000, n_pi=5000, n_po=5000, n_levels=400, p_fanin3=0.6, seed=0,
+               n_patterns=16384, faults="collapsed", hub_frac=0.1, biased_pi_frac=0.5,
+               p_one_biased=0.2),
+}
+
+
+def circuit(n_gates, n_pi, n_po, n_levels, p_fanin3=0.5, type_mask=BENCH_TYPES, seed=0,
+            window=4, hub_frac=0.0, hub_fo=(8, 64), fo=(1, 3), p_unused=0.5, shuffle_ids=True):
+    cfg = _lib.GenConfig(ctypes.sizeof(_lib.GenConfig), seed, n_gates, n_pi, n_po, n_levels,
+                         window, p_fanin3, type_mask, hub_frac, hub_fo[0], hub_fo[1], fo[0], fo[1],
+                         p_unused, 1 if shuffle_ids else 0)
+    ptr, n = ctypes.c_void_p(), ctypes.c_size_t()
+    _lib.check(_lib.lib().fsimb_gen_circuit(ctypes.byref(cfg), ctypes.byref(ptr), ctypes.byref(n)))
+    return _lib.take_text(ptr, n)
+
+
+def faults(ckt, kind="outputs"):
+    b = ckt.encode()
+    ptr, n = ctypes.c_void_p(), ctypes.c_size_t()
+    _lib.check(_lib.lib().fsimb_gen_faults(b, len(b), FAULT_KINDS[kind], ctypes.byref(ptr),
+                                           ctypes.byref(n)))
+    return _lib.take_text(ptr, n)
+
+
+def patterns(n_pi, n_patterns, seed=0, biased_pi_frac=0.0, p_one_biased=0.2):
+    ptr, n = ctypes.c_void_p(), ctypes.c_size_t()
+    _lib.check(_lib.lib().fsimb_gen_patterns(seed, n_patterns, n_pi, biased_pi_frac, p_one_biased,
+                                             ctypes.byref(ptr), ctypes.byref(n)))
+    return _lib.take_text(ptr, n)
+
+
+def generate(n_gates, n_pi, n_po, n_levels, n_patterns, faults="outputs", seed=0,
+             p_fanin3=0.5, type_mask=BENCH_TYPES, window=4, hub_frac=0.0, biased_pi_frac=0.0,
+             p_one_biased=0.2, pattern_seed=None):
+    """Returns {'ckt', 'flst', 'ptn'} texts for one seeded workload."""
+    ckt = circuit(n_gates, n_pi, n_po, n_levels, p_fanin3=p_fanin3, type_mask=type_mask,
+                  seed=seed, window=window, hub_frac=hub_frac)
+    fl = globals()["faults"](ckt, faults)
+    pt = patterns(n_pi, n_patterns, seed=seed if pattern_seed is None else pattern_seed,
+                  biased_pi_frac=biased_pi_frac, p_one_biased=p_one_biased)
+    return {"ckt": ckt, "flst": fl, "ptn": pt}
+
+
+def workload(name, **overrides):
+    cfg = dict(WORKLOADS[name])
+    cfg.update(overrides)
+    return generate(**cfg)

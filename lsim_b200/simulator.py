@@ -1,0 +1,220 @@
+"""Python mirror of LSIM's ``fsim::Simulator`` (fsim/simulation.hpp:39-188).
+
+Method names, argument meaning and error behaviour follow the reference:
+``read(ckt, flst, ptn)`` takes three paths or three text streams and raises
+``RuntimeError`` when a file cannot be opened (fsim/simulation.cpp:24-32);
+``run(mode, num_threads)`` simulates every round and fault; the accessors
+return the last round's good values, the ``found_fault_to_pattern`` table,
+the topological index map and the level counts.  Every mode runs on the B200
+through the C ABI; the reference's CPU modes are accepted for source
+compatibility and mean the same GPU run.
+
+Beyond the reference: ``results()`` returns, per fault, the detected flag,
+the first detecting pattern and the detection count over all patterns.
+"""
+import ctypes
+import enum
+import io
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import FsimbError, check
+
+RESULT_DTYPE = np.dtype([("detected", np.uint8), ("ref_last_round_flag", np.uint8),
+                         ("pad", np.uint8, 6), ("first_pattern", np.int64),
+                         ("count", np.uint64), ("ref_last_rd", np.uint64)])
+
+
+def _u64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+class Simulator:
+    class Mode(enum.IntEnum):
+        SEQUENTIAL = 0
+        PARALLEL_TF = 1
+        PARALLEL_OMP = 2
+        CUDA_B200 = 3
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(_lib.lib().fsimb_create(device, ctypes.byref(h)))
+        self._h = h
+        self._ran = False
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().fsimb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, code):
+        check(code, self._h)
+
+    # ------------------------------------------------------------ reading
+    def read(self, ckt, flst, ptn):
+        """Paths (str / PathLike) or text streams, like the two reference overloads."""
+        if all(isinstance(x, (str, os.PathLike)) for x in (ckt, flst, ptn)):
+            for p, what in ((ckt, "circut"), (flst, "fault"), (ptn, "pattern")):
+                if not os.path.isfile(p):
+                    raise RuntimeError("cannot open %s file %s" % (what, p))
+            self._check(_lib.lib().fsimb_load_files(self._h, os.fsencode(ckt), os.fsencode(flst),
+                                                    os.fsencode(ptn)))
+        else:
+            texts = [x.read() if isinstance(x, io.IOBase) or hasattr(x, "read") else x
+                     for x in (ckt, flst, ptn)]
+            self.read_text(*texts)
+        self._ran = False
+
+    def read_text(self, ckt, flst, ptn):
+        b = [t.encode() if isinstance(t, str) else bytes(t) for t in (ckt, flst, ptn)]
+        self._check(_lib.lib().fsimb_load_buffers(self._h, b[0], len(b[0]), b[1], len(b[1]),
+                                                  b[2], len(b[2])))
+        self._ran = False
+
+    def load_circuit(self, ckt):
+        b = ckt.encode() if isinstance(ckt, str) else bytes(ckt)
+        self._check(_lib.lib().fsimb_load_circuit(self._h, b, len(b)))
+
+    def set_fault_text(self, flst):
+        b = flst.encode() if isinstance(flst, str) else bytes(flst)
+        self._check(_lib.lib().fsimb_set_fault_text(self._h, b, len(b)))
+
+    def set_faults(self, site, pin, value):
+        site = np.ascontiguousarray(site, dtype=np.uint32)
+        pin = np.ascontiguousarray(pin, dtype=np.uint8)
+        value = np.ascontiguousarray(value, dtype=np.uint8)
+        n = len(site)
+        self._check(_lib.lib().fsimb_set_faults(
+            self._h, site.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+            pin.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            value.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n))
+
+    def set_patterns(self, words, num_patterns):
+        w = np.ascontiguousarray(words, dtype=np.uint64).ravel()
+        self._check(_lib.lib().fsimb_set_patterns(self._h, _u64p(w), int(num_patterns)))
+
+    # ------------------------------------------------------------ running
+    def run(self, mode=Mode.CUDA_B200, num_threads=1, drop=False, words_per_item=0,
+            block_threads=0, stream=None):
+        o = _lib.Opts(ctypes.sizeof(_lib.Opts), 1 if drop else 0, words_per_item, block_threads,
+                      stream)
+        self._check(_lib.lib().fsimb_run(self._h, ctypes.byref(o)))
+        self._ran = True
+
+    # ------------------------------------------------------------ results
+    def info(self):
+        i = _lib.Info()
+        self._check(_lib.lib().fsimb_get_info(self._h, ctypes.byref(i)))
+        return i
+
+    def stats(self):
+        s = _lib.Stats()
+        self._check(_lib.lib().fsimb_get_stats(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def results(self):
+        n = self.info().num_faults
+        out = np.zeros(n, dtype=RESULT_DTYPE)
+        self._check(_lib.lib().fsimb_results(
+            self._h, out.ctypes.data_as(ctypes.POINTER(_lib.FaultResult)), n))
+        return out
+
+    def found_fault_to_pattern(self):
+        n = 2 * self.info().num_faults
+        out = np.zeros(n, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_found_fault_to_pattern(self._h, _u64p(out), n))
+        return out
+
+    def good_values(self, round_=None):
+        i = self.info()
+        rd = i.num_rounds - 1 if round_ is None else round_
+        out = np.zeros(i.num_elements, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_good_values(self._h, rd, _u64p(out), i.num_elements))
+        return out
+
+    def g_pi_results(self):
+        return self.good_values()[: self.num_PIs()]
+
+    def g_gate_results(self):
+        return self.good_values()[self.num_PIs(): self.num_PIs() + self.num_gates()]
+
+    def g_po_results(self):
+        return self.good_values()[self.num_PIs() + self.num_gates():]
+
+    # ------------------------------------------------------------ accessors
+    def num_PIs(self):
+        return self.info().num_pis
+
+    def num_POs(self):
+        return self.info().num_pos
+
+    num_pos = num_POs
+
+    def num_gates(self):
+        return self.info().num_gates
+
+    def num_wires(self):
+        return self.info().num_wires
+
+    def num_rounds(self):
+        return self.info().num_rounds
+
+    def gate_idx_to_tpg_order_idx(self):
+        n = self.info().num_elements
+        out = np.zeros(n, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_topo_map(self._h, _u64p(out), n))
+        return out
+
+    def levels(self):
+        n = self.info().num_elements
+        out = np.zeros(n, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_levels(self._h, _u64p(out), n))
+        return out
+
+    def num_gates_per_level(self):
+        n = self.info().num_levels
+        out = np.zeros(n, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_gates_per_level(self._h, _u64p(out), n))
+        return out
+
+    def types(self):
+        n = self.info().num_elements
+        out = np.zeros(n, dtype=np.uint8)
+        self._check(_lib.lib().fsimb_types(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n))
+        return out
+
+    def faults(self):
+        """(site, pin, value) arrays; site is the topological index."""
+        n = self.info().num_faults
+        s = np.zeros(n, dtype=np.uint32)
+        p = np.zeros(n, dtype=np.uint8)
+        v = np.zeros(n, dtype=np.uint8)
+        self._check(_lib.lib().fsimb_faults(
+            self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+            p.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            v.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n))
+        return s, p, v
+
+    def patterns(self):
+        i = self.info()
+        out = np.zeros(i.num_rounds * i.num_pis, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_patterns(self._h, _u64p(out), len(out)))
+        return out.reshape(i.num_rounds, i.num_pis)
+
+
+__all__ = ["Simulator", "FsimbError", "RESULT_DTYPE"]
