@@ -332,7 +332,21 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
+    ap.add_argument("--profile", action="store_true",
+                    help="one untimed run of the workload (for profiler captures)")
     args = ap.parse_args()
+    if args.profile:
+        from lsim_b200 import Simulator, gen
+        w = gen.workload(args.workload)
+        sim = Simulator(0)
+        sim.read_text(w["ckt"], w["flst"], w["ptn"])
+        for _ in range(max(1, args.steps)):
+            sim.run()
+        st = sim.stats()
+        print(json.dumps({"workload": args.workload, "faults": sim.info().num_faults,
+                          "patterns": sim.info().num_patterns, "stats": st}))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

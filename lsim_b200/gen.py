@@ -32,6 +32,10 @@ WORKLOADS = {
                n_patterns=4096, faults="outputs"),
     "c2": dict(n_gates=200000, n_pi=1000, n_po=1000, n_levels=150, p_fanin3=0.6, seed=0,
                n_patterns=65536, faults="collapsed"),
+    # c2 shape (same level width, fan-in and fault model), 50,000 gates, one
+    # 2,048-pattern tile: the profiling case for the sweep kernel
+    "c2s": dict(n_gates=50000, n_pi=1000, n_po=1000, n_levels=38, p_fanin3=0.6, seed=0,
+                n_patterns=2048, faults="collapsed"),
     "c3": dict(n_gates=2000000, n_pi=5000, n_po=5000, n_levels=400, p_fanin3=0.6, seed=0,
                n_patterns=16384, faults="collapsed", hub_frac=0.1, biased_pi_frac=0.5,
                p_one_biased=0.2),
