@@ -147,6 +147,27 @@ int fsimb_faults(const fsimb_handle* h, uint32_t* site, uint8_t* pin, uint8_t* v
 /* loaded pattern words, n = rounds * nPI */
 int fsimb_patterns(const fsimb_handle* h, uint64_t* out, uint64_t n);
 
+/* Good-machine PO words without allocating device memory.  This entry point
+ * has no counterpart in the reference.  It serves callers that may not call
+ * cudaMalloc/cudaFree (or any allocating routine) at this point: code that
+ * runs under a device-memory budget fixed up front, or a serving loop that
+ * cannot take the device-wide synchronisation those calls imply.
+ *   d_pattern_words  device array [n_words][nPI], round-major like .ptn rows
+ *   n_words          1..32 pattern words (up to 2048 patterns)
+ *   d_po_words       device array [n_words][nPO]: good-machine PO words, not
+ *                    masked to a partial round's valid bits
+ * The element values live in one static device array that holds circuits of
+ * up to 32,768 elements (8 MiB on every GPU that loads the library, kept until
+ * the process exits); larger circuits fail with FSIMB_ERR_LIMIT.  The circuit
+ * must already be on the device (after one fsimb_run on h).  The first call
+ * on a device looks up the array's device address once: make that first call
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents; every value is written before it is read, so nothing needs
+ * clearing, but calls whose kernels overlap on the GPU race on it.  Returns
+ * after the kernels are enqueued on `stream` (NULL: the handle's stream). */
+int fsimb_good_po_noalloc(fsimb_handle* h, const uint64_t* d_pattern_words, uint32_t n_words,
+                          uint64_t* d_po_words, void* stream);
+
 /* Synthetic workloads (seeded; text in LSIM's formats).  Returned buffers
  * are released with fsimb_free_text. */
 typedef struct {

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <string>
@@ -912,3 +913,109 @@ int fsimb_gen_patterns(uint64_t seed, uint64_t n_patterns, uint64_t n_pi, double
 void fsimb_free_text(char* text) { std::free(text); }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ no-allocation
+// Good-machine PO words for up to one tile of pattern words, for callers that
+// must not allocate device memory on the call (for example code running under
+// a fixed device-memory budget handed out up front, or a serving loop that may
+// not take the implicit device synchronisation of cudaMalloc/cudaFree).  The
+// element values, which the regular path keeps in a buffer sized per circuit,
+// live here in one file-scope device array of fixed size, shared by every call
+// on a device.
+namespace {
+
+constexpr uint32_t kNoAllocMaxElements = 32768;  // 32,768 elements x 32 words x 8 B = 8 MiB
+static __device__ __align__(256) uint64_t g_noalloc_values[(size_t)kNoAllocMaxElements * kTileWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint64_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+__global__ void k_good_level_static(const uint8_t* type, const uint32_t* fi_off,
+                                    const uint32_t* fi_idx, const uint64_t* pwords,
+                                    uint32_t n_words, uint32_t n_pi, uint32_t po_begin,
+                                    uint32_t n_po, uint32_t lo, uint32_t hi, uint64_t* vals,
+                                    uint64_t* po_out) {
+  const uint32_t n = (hi - lo) * kTileWords;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    const uint32_t lane = idx % kTileWords;
+    const uint32_t e = lo + idx / kTileWords;
+    const uint8_t t = type[e];
+    uint64_t v;
+    if (t == G_PI) {
+      v = lane < n_words ? pwords[(uint64_t)lane * n_pi + e] : 0ull;
+    } else {
+      const uint32_t f0 = fi_off[e];
+      uint32_t nf = fi_off[e + 1] - f0;
+      if (t == G_INV || t == G_CLKBUF || t == G_PO) nf = 1;
+      uint64_t in[4] = {0, 0, 0, 0};
+      for (uint32_t k = 0; k < nf && k < 4; ++k) in[k] = vals[(uint64_t)fi_idx[f0 + k] * kTileWords + lane];
+      uint64_t r = in[0];
+      switch (t) {
+        case G_INV: r = ~r; break;
+        case G_AND: case G_NAND:
+          for (uint32_t k = 1; k < nf; ++k) r &= in[k];
+          if (t == G_NAND) r = ~r;
+          break;
+        case G_OR: case G_NOR:
+          for (uint32_t k = 1; k < nf; ++k) r |= in[k];
+          if (t == G_NOR) r = ~r;
+          break;
+        case G_XOR: case G_XNOR:
+          for (uint32_t k = 1; k < nf; ++k) r ^= in[k];
+          if (t == G_XNOR) r = ~r;
+          break;
+        case G_MUX: r = (in[2] & in[1]) | (in[0] & (uint64_t)(in[2] == 0)); break;
+        default: break;  // CLKBUF, PO: copy
+      }
+      v = r;
+    }
+    vals[(uint64_t)e * kTileWords + lane] = v;
+    if (e >= po_begin && e - po_begin < n_po && lane < n_words)
+      po_out[(uint64_t)lane * n_po + (e - po_begin)] = v;
+  }
+}
+
+// Address of the static array on the current device, looked up once per
+// device (host code cannot use the array's name as a device address).
+uint64_t* noalloc_scratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) throw ArgError{"device index out of range"};
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_values));
+    g_noalloc_ptr[device] = (uint64_t*)p;
+  }
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" int fsimb_good_po_noalloc(fsimb_handle* h, const uint64_t* d_pattern_words,
+                                     uint32_t n_words, uint64_t* d_po_words, void* stream) {
+  API_BEGIN(h)
+  if (h->device < 0) throw CudaError{"host-only handle: no GPU to run on"};
+  if (!h->has_ckt || !h->plan_uploaded)
+    throw StateError{"the circuit is not on the device yet: call fsimb_run once first"};
+  if (n_words == 0 || n_words > kTileWords) throw ArgError{"n_words must be in 1..32"};
+  if (!d_pattern_words || !d_po_words) throw ArgError{"null device pointer"};
+  if (h->nl.N > kNoAllocMaxElements)
+    throw LimitError{"circuit has " + std::to_string(h->nl.N) + " elements; the no-allocation "
+                     "entry point holds at most " + std::to_string(kNoAllocMaxElements)};
+  CK(cudaSetDevice(h->device));
+  uint64_t* vals = noalloc_scratch(h->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  const uint32_t po_begin = (uint32_t)(h->nl.n_pi + h->nl.n_gates);
+  for (uint32_t l = 0; l < h->nl.n_levels; ++l) {
+    const uint32_t lo = h->nl.level_off[l], hi = h->nl.level_off[l + 1];
+    if (hi == lo) continue;
+    const uint32_t n = (hi - lo) * kTileWords;
+    const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148u * 16u);
+    k_good_level_static<<<blocks, 256, 0, s>>>(h->d_type.as<uint8_t>(), h->d_fi_off.as<uint32_t>(),
+                                                h->d_fi_idx.as<uint32_t>(), d_pattern_words, n_words,
+                                                (uint32_t)h->nl.n_pi, po_begin, (uint32_t)h->nl.n_po,
+                                                lo, hi, vals, d_po_words);
+  }
+  CK(cudaGetLastError());
+  API_END(h)
+}
