@@ -53,7 +53,7 @@ typedef struct {
                                 after the 2048-pattern tile that first detects
                                 it (first_pattern exact, count covers that tile) */
   uint32_t words_per_item;   /* sweep words per work item: 0 auto, or 1,2,4,8 */
-  uint32_t block_threads;    /* sweep CTA size: 0 auto, or 32..512 */
+  uint32_t block_threads;    /* sweep CTA size: 0 auto, or a multiple of 32 up to 1024 */
   void* stream;              /* cudaStream_t to run on; NULL: the handle's stream */
 } fsimb_opts;
 
@@ -84,6 +84,8 @@ typedef struct {
   uint64_t device_bytes;     /* device memory held by the handle */
   uint64_t kernel_launches;  /* kernels launched by the last run */
   double ms_compute;         /* device time from results init to the last tile */
+  uint64_t bank_conflict_groups; /* sweep access groups whose slots share a bank position */
+  uint64_t bank_access_groups;   /* sweep access groups (fanin loads and stores) per item */
 } fsimb_stats;
 
 /* Lifecycle.  fsimb_create fails with FSIMB_ERR_CUDA when `device` is not a

@@ -52,7 +52,8 @@ class Stats(ctypes.Structure):
                 [(n, ctypes.c_uint32) for n in
                  ["words_per_item", "block_threads", "blocks", "smem_bytes"]] +
                 [("device_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
-                 ("ms_compute", ctypes.c_double)])
+                 ("ms_compute", ctypes.c_double), ("bank_conflict_groups", ctypes.c_uint64),
+                 ("bank_access_groups", ctypes.c_uint64)])
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -115,10 +115,13 @@ struct fsimb_handle {
   Plan plan;
   bool plan_valid = false;
   bool plan_uploaded = false;
+  Schedule sched;          // for sched_M words per item
+  int sched_M = 0;
+  bool sched_uploaded = false;
 
-  DevBuf d_type, d_fi_off, d_fi_idx, d_fslot, d_meta, d_level, d_level_off, d_li_off, d_li_elem;
+  DevBuf d_type, d_fi_off, d_fi_idx, d_recs, d_level, d_level_off, d_li_off, d_li;
   DevBuf d_roots, d_members, d_traced, d_inj, d_exact;
-  DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue;
+  DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue, d_err;
   DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout;
   uint64_t good_tiles = 0;  // tiles held in d_good
   uint64_t good_P = 0;
@@ -132,10 +135,10 @@ struct fsimb_handle {
   ~fsimb_handle() {
     if (device >= 0) {
       cudaSetDevice(device);
-      for (DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_fslot, &d_meta, &d_level, &d_level_off,
-                        &d_li_off, &d_li_elem, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+      for (DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
+                        &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                         &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
-                        &d_queue, &d_root_list[0], &d_root_list[1], &d_sweep_list,
+                        &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
                         &d_exact_list[0], &d_exact_list[1], &d_nout})
         b->release();
       for (auto e : events) cudaEventDestroy(e);
@@ -154,10 +157,10 @@ struct fsimb_handle {
 
   uint64_t device_bytes() const {
     uint64_t s = 0;
-    for (const DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_fslot, &d_meta, &d_level, &d_level_off,
-                            &d_li_off, &d_li_elem, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+    for (const DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
+                            &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                             &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
-                            &d_queue, &d_root_list[0], &d_root_list[1], &d_sweep_list,
+                            &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
                             &d_exact_list[0], &d_exact_list[1], &d_nout})
       s += b->n;
     return s;
@@ -168,6 +171,8 @@ struct fsimb_handle {
     has_pats = false;
     plan_valid = false;
     plan_uploaded = false;
+    sched_M = 0;
+    sched_uploaded = false;
     has_results = false;
     good_tiles = 0;
   }
@@ -218,8 +223,8 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (o.words_per_item && o.words_per_item != 1 && o.words_per_item != 2 && o.words_per_item != 4 &&
       o.words_per_item != 8)
     throw ArgError{"words_per_item must be 0, 1, 2, 4 or 8"};
-  if (o.block_threads && (o.block_threads < 32 || o.block_threads > 512 || o.block_threads % 32))
-    throw ArgError{"block_threads must be 0 or a multiple of 32 in 32..512"};
+  if (o.block_threads && (o.block_threads < 32 || o.block_threads > 1024 || o.block_threads % 32))
+    throw ArgError{"block_threads must be 0 or a multiple of 32 in 32..1024"};
   CK(cudaSetDevice(device));
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : stream;
   has_results = false;
@@ -228,6 +233,8 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     build_plan(nl, faults, plan);
     plan_valid = true;
     plan_uploaded = false;
+    sched_M = 0;
+    sched_uploaded = false;
   }
   const uint32_t N = plan.N;
   const uint64_t F = faults.size();
@@ -240,25 +247,66 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (W_pad > (1ull << 31) || tiles * (uint64_t)N * kTileWords > (1ull << 40))
     throw LimitError{"pattern block too large"};
 
-  // Sweep shape: M words per item, CTA size, CTAs per SM.
+  // Sweep shape: M words per item (the largest whose slots fit in shared
+  // memory), a schedule for residue groups of 16/M, two record staging
+  // buffers in the rest, and the CTA size.
   const size_t static_smem = 256;
   const size_t budget = smem_optin > static_smem + 1024 ? smem_optin - static_smem - 1024 : 0;
   int M = (int)o.words_per_item;
+  const bool fixed_M = M != 0;
   if (!M) {
     M = 8;
     while (M > 1 && (size_t)plan.max_live * M * 8 > budget) M /= 2;
-    // keep at least ~4 items per SM in flight for narrow circuits
   }
-  const size_t smem = std::max<size_t>(16, (size_t)plan.max_live * M * 8);
-  if (smem > budget)
-    throw LimitError{"a sweep needs " + std::to_string(plan.max_live) +
-                     " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
-                     " at " + std::to_string(M) + " word(s) per item"};
+  for (;;) {
+    if (sched_M != M) {
+      build_schedule(nl, plan, 16u / (uint32_t)M, sched);
+      sched_M = M;
+      sched_uploaded = false;
+    }
+    const bool fits = sched.max_live <= kMaxSlots && (size_t)sched.max_live * M * 8 <= budget;
+    if (fits) break;
+    if (fixed_M || M == 1)
+      throw LimitError{"a sweep needs " + std::to_string(sched.max_live) +
+                       " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
+                       " at " + std::to_string(M) + " word(s) per item"};
+    M /= 2;
+  }
+  const size_t vals_bytes = ((size_t)sched.max_live * M * 8 + 15) / 16 * 16;
+  uint32_t widest = 1;
+  std::vector<uint32_t> widths;
+  for (uint32_t l = 1; l <= plan.max_gate_level && l < plan.n_levels; ++l) {
+    widths.push_back(plan.level_off[l + 1] - plan.level_off[l]);
+    widest = std::max(widest, widths.back());
+  }
+  const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (budget - vals_bytes) / 32);
+  const size_t smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
+  // CTA size: one thread per gate of a level; the multiple of 32 that splits
+  // the typical (90th percentile) level width into equal rounds, so no
+  // thread idles long before the per-level barrier.
+  const uint32_t tmax = M >= 8 ? 512 : (M >= 4 ? 768 : 1024);
   int threads = (int)o.block_threads;
   if (!threads) {
-    uint32_t w = std::max<uint32_t>(plan.max_level_width, 1);
-    threads = (int)std::min<uint32_t>(512, std::max<uint32_t>(64, (w + 31) / 32 * 32));
+    uint32_t w = 64;
+    if (!widths.empty()) {
+      std::nth_element(widths.begin(), widths.begin() + widths.size() * 9 / 10, widths.end());
+      w = std::max<uint32_t>(widths[widths.size() * 9 / 10], 1);
+    }
+    uint32_t best = 64;
+    double best_cost = 1e30;
+    for (uint32_t k = 1; k <= 64; ++k) {
+      uint32_t t = (w + k - 1) / k;
+      t = std::max<uint32_t>(64, (t + 31) / 32 * 32);
+      if (t > tmax) continue;
+      const double cost = (double)k * t + 8.0 * k;  // issued slots + per-round overhead
+      if (cost < best_cost) {
+        best_cost = cost;
+        best = t;
+      }
+    }
+    threads = (int)best;
   }
+  threads = std::min<int>(threads, (int)tmax);
 
   cudaEvent_t e0 = ev(0), e1 = ev(1), e2 = ev(2), e3 = ev(3);
   CK(cudaEventRecord(e0, s));
@@ -266,18 +314,20 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     upload(d_type, nl.type, s);
     upload(d_fi_off, nl.fi_off, s);
     upload(d_fi_idx, nl.fi_idx, s);
-    upload(d_fslot, plan.fslot, s);
-    upload(d_meta, plan.meta, s);
     upload(d_level, nl.level, s);
     upload(d_level_off, plan.level_off, s);
-    upload(d_li_off, plan.li_off, s);
-    upload(d_li_elem, plan.li_elem, s);
     upload(d_roots, plan.roots, s);
     upload(d_members, plan.members, s);
     upload(d_traced, plan.traced, s);
     upload(d_inj, plan.sweeps, s);
     upload(d_exact, plan.exact_fault, s);
     plan_uploaded = true;
+  }
+  if (!sched_uploaded) {
+    upload(d_recs, sched.recs, s);
+    upload(d_li_off, sched.li_off, s);
+    upload(d_li, sched.li, s);
+    sched_uploaded = true;
   }
   if (!pats_uploaded) {
     upload(d_pwords, pats.words, s);
@@ -291,6 +341,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   d_first.ensure(std::max<uint64_t>(F, 1) * 8);
   d_lastflag.ensure(std::max<uint64_t>(F, 1));
   d_queue.ensure(std::max<uint64_t>(tiles, 1) * sizeof(int));
+  d_err.ensure(sizeof(int));
   if (o.drop) {
     d_root_list[0].ensure(std::max<uint32_t>(n_roots, 1) * 4);
     d_root_list[1].ensure(std::max<uint32_t>(n_roots, 1) * 4);
@@ -300,6 +351,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     d_nout.ensure(16);
   }
   CK(cudaMemsetAsync(d_queue.p, 0, std::max<uint64_t>(tiles, 1) * sizeof(int), s));
+  CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
   launch_init_results(d_count.as<unsigned long long>(), d_first.as<unsigned long long>(),
                       d_lastflag.as<uint8_t>(), (uint32_t)F, s);
   CK(cudaEventRecord(e1, s));
@@ -348,12 +400,11 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     CK(cudaEventRecord(a0, s));
     if (n_sw) {
       SweepArgs sa{};
-      sa.fslot = d_fslot.as<uint4>();
-      sa.meta = d_meta.as<uint32_t>();
+      sa.recs = d_recs.as<uint4>();
       sa.level = d_level.as<uint32_t>();
       sa.level_off = d_level_off.as<uint32_t>();
       sa.li_off = d_li_off.as<uint32_t>();
-      sa.li_elem = d_li_elem.as<uint32_t>();
+      sa.li = d_li.as<uint32_t>();
       sa.fi_off = d_fi_off.as<uint32_t>();
       sa.fi_idx = d_fi_idx.as<uint32_t>();
       sa.type = d_type.as<uint8_t>();
@@ -366,6 +417,9 @@ void fsimb_handle::run(const fsimb_opts* opts) {
       sa.good = good_t;
       sa.out = d_out.as<uint64_t>();
       sa.queue = d_queue.as<int>() + t;
+      sa.vals_bytes = (uint32_t)vals_bytes;
+      sa.rec_buf = rec_buf;
+      sa.err = d_err.as<int>();
       const int nb = (int)std::min<uint64_t>((uint64_t)blocks, (uint64_t)n_sw * sa.subtiles);
       CK(launch_sweep(M, threads, nb, smem, sa, s));
       ++launches;
@@ -479,7 +533,9 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   // 4. results
   std::vector<unsigned long long> cnt(F), fst(F);
   std::vector<uint8_t> lf(F);
+  int kerr = 0;
   cudaEvent_t e4 = ev(4 + 3 * tiles + 1);
+  CK(cudaMemcpyAsync(&kerr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   if (F) {
     CK(cudaMemcpyAsync(cnt.data(), d_count.p, F * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(fst.data(), d_first.p, F * 8, cudaMemcpyDeviceToHost, s));
@@ -487,6 +543,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   }
   CK(cudaEventRecord(e4, s));
   CK(cudaStreamSynchronize(s));
+  if (kerr) throw CudaError{"a sweep kernel reached its wait limit for a record copy; results discarded"};
   if (!o.drop) {
     for (uint64_t t = 0; t < tiles; ++t) {
       float x = 0;
@@ -532,7 +589,9 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   CK(cudaEventElapsedTime(&x, e1, e3));
   stats.ms_compute = x;
   stats.good_gate_words = (uint64_t)(N - plan.n_pi) * W_pad;
-  stats.max_live = plan.max_live;
+  stats.max_live = sched.max_live;
+  stats.bank_conflict_groups = sched.conflict_groups;
+  stats.bank_access_groups = sched.access_groups;
   stats.words_per_item = (uint32_t)M;
   stats.block_threads = (uint32_t)threads;
   stats.blocks = (uint32_t)blocks;

@@ -6,7 +6,8 @@
 //   k_sweep<M>     persistent: each CTA pulls (sweep, M-word subtile) items from
 //                  a device work counter and re-simulates the levels above the
 //                  injection point with all live values in shared memory
-//                  (slots assigned on the host by interval allocation).  Writes
+//                  (slots and a bank-conflict-free order chosen on the host;
+//                  gate records staged per level by TMA bulk copies).  Writes
 //                  the OR over POs of (faulty ^ good) per word.
 //   k_ffr          one warp per FFR root, lanes = the 32 words of a tile:
 //                  backward critical-path tracing inside the FFR and the
@@ -89,36 +90,48 @@ __global__ void k_good_level(GoodArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- TMA bulk staging
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// One thread arms the barrier for `bytes` and starts a bulk copy (no
+// multicast) of `bytes` from global to this CTA's shared memory.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  if (bytes == 0) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+    return;
+  }
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Waits for the barrier's phase `parity` with an iteration limit; false if
+// the limit was reached (the caller reports the error instead of hanging).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------- sweep
-template <int M>
-__device__ __forceinline__ void ld_words(const uint64_t* p, uint64_t (&v)[M]) {
-  if constexpr (M == 1) {
-    v[0] = p[0];
-  } else {
-#pragma unroll
-    for (int i = 0; i < M / 2; ++i) {
-      ulonglong2 q = reinterpret_cast<const ulonglong2*>(p)[i];
-      v[2 * i] = q.x;
-      v[2 * i + 1] = q.y;
-    }
-  }
-}
-
-template <int M>
-__device__ __forceinline__ void st_words(uint64_t* p, const uint64_t (&v)[M]) {
-  if constexpr (M == 1) {
-    p[0] = v[0];
-  } else {
-#pragma unroll
-    for (int i = 0; i < M / 2; ++i)
-      reinterpret_cast<ulonglong2*>(p)[i] = make_ulonglong2(v[2 * i], v[2 * i + 1]);
-  }
-}
-
 // Faulty value of the injection element for word w of the tile.
 __device__ __forceinline__ uint64_t inj_value(const SweepArgs& a, const InjRec& inj, uint32_t w) {
   const uint32_t x = inj.elem;
-  if (inj.mode == 0) return ~a.good[(uint64_t)x * 32 + w];
+  if (!(inj.mode & kInjStuck)) return ~a.good[(uint64_t)x * 32 + w];
   const uint64_t sv = inj.value ? ~0ull : 0ull;
   if (inj.pin == 0) return sv;
   const uint8_t t = a.type[x];
@@ -137,12 +150,167 @@ __device__ __forceinline__ uint64_t inj_value(const SweepArgs& a, const InjRec& 
 }
 
 template <int M>
-__global__ void __launch_bounds__(512) k_sweep(SweepArgs a) {
-  extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M]
+__device__ __forceinline__ void lds_chunk(const uint64_t* vals, uint32_t slot, int h, uint64_t (&v)[2]) {
+  if constexpr (M == 1) {
+    v[0] = vals[slot];
+  } else {
+    const ulonglong2 q = *reinterpret_cast<const ulonglong2*>(vals + (size_t)slot * M + 2 * h);
+    v[0] = q.x;
+    v[1] = q.y;
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void sts_chunk(uint64_t* vals, uint32_t slot, int h, const uint64_t (&v)[2]) {
+  if constexpr (M == 1)
+    vals[slot] = v[0];
+  else
+    *reinterpret_cast<ulonglong2*>(vals + (size_t)slot * M + 2 * h) = make_ulonglong2(v[0], v[1]);
+}
+
+template <int M>
+using PoAcc = uint64_t[(M >= 2) ? M / 2 : 1][(M >= 2) ? 2 : 1];
+
+// One gate of a known class (family F, fan-in NF) on all M words of the item:
+// loads of the fanin chunks, the gate function, the store and the PO
+// difference.  F = 0: io ^ AND(in ^ ii) covers AND, NAND, OR, NOR, INV and
+// CLKBUF; F = 1: io ^ XOR(in) covers XOR and XNOR; F = 2: MUX.  Each class is
+// its own code path, selected by one branch per gate (gates are ordered by
+// class, so the branch is warp-uniform).  Loads and stores sit inside the
+// class bodies so that the branch stays a branch.
+template <int M, int F, int NF>
+__device__ __forceinline__ void gate_body(uint64_t* vals, const uint4 q, uint32_t meta, int pl,
+                                          const uint64_t* good_row, PoAcc<M>& pacc) {
+  constexpr int C = (M >= 2) ? M / 2 : 1;
+  constexpr int VC = (M >= 2) ? 2 : 1;
+  const uint32_t t = meta & kRecTypeMask;
+  const uint64_t ii = bmask((kIiMask >> t) & 1u);
+  const uint64_t io = bmask((kIoMask >> t) & 1u);
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int h = (pl + c) % C;
+    uint64_t i0[2], i1[2] = {0, 0}, i2[2] = {0, 0}, i3[2] = {0, 0};
+    lds_chunk<M>(vals, q.x & 0xFFFFu, h, i0);
+    if constexpr (NF > 1) lds_chunk<M>(vals, q.x >> 16, h, i1);
+    if constexpr (NF > 2) lds_chunk<M>(vals, q.y & 0xFFFFu, h, i2);
+    if constexpr (NF > 3) lds_chunk<M>(vals, q.y >> 16, h, i3);
+    uint64_t r[2];
+#pragma unroll
+    for (int v = 0; v < VC; ++v) {
+      uint64_t x;
+      if constexpr (F == 0) {
+        x = i0[v] ^ ii;
+        if constexpr (NF > 1) x &= i1[v] ^ ii;
+        if constexpr (NF > 2) x &= i2[v] ^ ii;
+        if constexpr (NF > 3) x &= i3[v] ^ ii;
+        x ^= io;
+      } else if constexpr (F == 1) {
+        x = i0[v];
+        if constexpr (NF > 1) x ^= i1[v];
+        if constexpr (NF > 2) x ^= i2[v];
+        if constexpr (NF > 3) x ^= i3[v];
+        x ^= io;
+      } else {
+        // (s & b) | (a & !s) with a logical not (fsim/simulation.cpp:1056)
+        x = (i2[v] & i1[v]) | (i0[v] & (uint64_t)(i2[v] == 0));
+      }
+      r[v] = x;
+    }
+    if (meta & kRecHasSlot) sts_chunk<M>(vals, q.z & 0xFFFFu, h, r);
+    if (meta & kRecPo) {
+#pragma unroll
+      for (int v = 0; v < VC; ++v) pacc[c][v] |= r[v] ^ good_row[VC * h + v];
+    }
+  }
+}
+
+// Any other class (rare combinations): word-by-word generic evaluation.
+template <int M>
+__device__ __forceinline__ void gate_generic(uint64_t* vals, const uint4 q, uint32_t meta, int pl,
+                                             const uint64_t* good_row, PoAcc<M>& pacc) {
+  constexpr int C = (M >= 2) ? M / 2 : 1;
+  constexpr int VC = (M >= 2) ? 2 : 1;
+  const uint32_t t = meta & kRecTypeMask;
+  const uint32_t nf = ((meta >> kRecNfShift) & 3u) + 1u;
+  for (int c = 0; c < C; ++c) {
+    const int h = (pl + c) % C;
+    uint64_t i0[2], i1[2] = {0, 0}, i2[2] = {0, 0}, i3[2] = {0, 0};
+    lds_chunk<M>(vals, q.x & 0xFFFFu, h, i0);
+    if (nf > 1) lds_chunk<M>(vals, q.x >> 16, h, i1);
+    if (nf > 2) lds_chunk<M>(vals, q.y & 0xFFFFu, h, i2);
+    if (nf > 3) lds_chunk<M>(vals, q.y >> 16, h, i3);
+    uint64_t r[2];
+    for (int v = 0; v < VC; ++v) r[v] = eval_word(t, nf, i0[v], i1[v], i2[v], i3[v]);
+    if (meta & kRecHasSlot) sts_chunk<M>(vals, q.z & 0xFFFFu, h, r);
+    if (meta & kRecPo)
+      for (int v = 0; v < VC; ++v) pacc[c][v] |= r[v] ^ good_row[VC * h + v];
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void gate_dispatch(uint64_t* vals, const uint4 q, int pl,
+                                              const uint64_t* good_row, PoAcc<M>& pacc) {
+  const uint32_t meta = q.z >> 16;
+  const uint32_t t = meta & kRecTypeMask;
+  const uint32_t fam = ((kXfMask >> t) & 1u) | (t == G_MUX ? 2u : 0u);
+  const uint32_t code = fam * 4 + ((meta >> kRecNfShift) & 3u);  // family, fan-in - 1
+  switch (code) {
+    case 0: gate_body<M, 0, 1>(vals, q, meta, pl, good_row, pacc); break;
+    case 1: gate_body<M, 0, 2>(vals, q, meta, pl, good_row, pacc); break;
+    case 2: gate_body<M, 0, 3>(vals, q, meta, pl, good_row, pacc); break;
+    case 3: gate_body<M, 0, 4>(vals, q, meta, pl, good_row, pacc); break;
+    case 5: gate_body<M, 1, 2>(vals, q, meta, pl, good_row, pacc); break;
+    case 6: gate_body<M, 1, 3>(vals, q, meta, pl, good_row, pacc); break;
+    case 7: gate_body<M, 1, 4>(vals, q, meta, pl, good_row, pacc); break;
+    case 10: gate_body<M, 2, 3>(vals, q, meta, pl, good_row, pacc); break;
+    default: gate_generic<M>(vals, q, meta, pl, good_row, pacc); break;
+  }
+}
+
+// M words per item, one thread per gate holding all M words.  Slots are
+// M*8 bytes; a thread reads a slot as C = M/2 16-byte chunks (one 8-byte word
+// for M = 1).  The host orders each level in groups of G = 16/M consecutive
+// positions whose slots have distinct residues mod G (for every fanin and the
+// output).  Within a phase of 8 lanes (16 for M = 1), lane l takes position
+// (l % C) * G + l / C and reads chunk (l + i) % C at step i, so the 8 chunks a
+// phase touches lie in 8 different bank quads: the loads and stores of a
+// sweep are free of bank conflicts wherever the host found such groups.
+//
+// Gate records are staged per level into two shared-memory buffers by TMA
+// bulk copies issued two levels ahead (one elected thread, mbarrier
+// completion); a level wider than a buffer reads the rest from global.
+template <int M>
+__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(SweepArgs a) {
+  constexpr int C = (M >= 2) ? M / 2 : 1;   // chunks per slot
+  constexpr int VC = (M >= 2) ? 2 : 1;      // words per chunk
+  constexpr int G = 16 / M;                 // residue group size
+  constexpr int PH = (M == 1) ? 16 : 8;     // lanes per shared-memory phase
+  extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M] | recbuf[2][rec_buf]
   __shared__ unsigned long long acc[M];
+  __shared__ __align__(8) uint64_t bars[2];
   __shared__ int s_item;
   const int tid = threadIdx.x, nth = blockDim.x;
+  const int pl = tid & (PH - 1);
+  const uint32_t my_off = (uint32_t)((tid & ~(PH - 1)) + ((M >= 2) ? (pl % C) * G + pl / C : pl));
   const uint32_t n_items = a.n_list * a.subtiles;
+  const uint32_t Lmax = a.max_gate_level;
+  uint4* recbuf = reinterpret_cast<uint4*>(reinterpret_cast<char*>(vals) + a.vals_bytes);
+  // Zeroed buffers: a record read before its copy landed names slot 0 and
+  // element 0, both in range.
+  for (uint32_t i = tid; i < 2 * a.rec_buf; i += nth) recbuf[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t phase0 = 0, phase1 = 0;
+  auto stage = [&](uint32_t L, int b) {  // thread 0 only
+    const uint32_t lo = a.level_off[L], hi = a.level_off[L + 1];
+    const uint32_t n = min(hi - lo, a.rec_buf);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bulk_load(recbuf + (size_t)b * a.rec_buf, a.recs + lo, n * 16u, &bars[b]);
+  };
   for (;;) {
     if (tid == 0) s_item = atomicAdd(a.queue, 1);
     if (tid < M) acc[tid] = 0ull;
@@ -155,60 +323,71 @@ __global__ void __launch_bounds__(512) k_sweep(SweepArgs a) {
     const InjRec inj = a.inj[si];
     const uint32_t x = inj.elem;
     const uint32_t L0 = a.level[x] + 1;
-    const uint32_t xmeta = a.meta[x];
-    // Values live at the start level come from the good machine, except the
-    // injection element itself.
-    if (L0 <= a.max_gate_level) {
+    if (tid == 0 && L0 <= Lmax) {
+      stage(L0, 0);
+      if (L0 + 1 <= Lmax) stage(L0 + 1, 1);
+    }
+    uint32_t lo = 0, hi = 0;
+    if (L0 <= Lmax) {
+      lo = a.level_off[L0];
+      hi = a.level_off[L0 + 1];
+      // Values live at the start level come from the good machine, except
+      // the injection element itself.
       const uint32_t i1 = a.li_off[L0 + 1];
       for (uint32_t i = a.li_off[L0] + tid; i < i1; i += nth) {
-        const uint32_t e = a.li_elem[i];
-        const uint32_t slot = a.meta[e] & kMetaSlotMask;
-        uint64_t v[M];
-        if (e == x) {
+        const uint2 es = reinterpret_cast<const uint2*>(a.li)[i];
+        uint64_t* dst = vals + (size_t)es.y * M;
+        if (es.x == x) {
 #pragma unroll
-          for (int m = 0; m < M; ++m) v[m] = inj_value(a, inj, w0 + m);
+          for (int m = 0; m < M; ++m) dst[m] = inj_value(a, inj, w0 + m);
         } else {
-          ld_words<M>(a.good + (uint64_t)e * 32 + w0, v);
+          const uint64_t* src = a.good + (uint64_t)es.x * 32 + w0;
+#pragma unroll
+          for (int m = 0; m < M; ++m) dst[m] = src[m];
         }
-        st_words<M>(vals + (size_t)slot * M, v);
       }
     }
-    if (tid < M && ((xmeta & kMetaPo) || a.type[x] == G_PO)) {
-      const uint32_t w = w0 + tid;
-      acc[tid] = inj_value(a, inj, w) ^ a.good[(uint64_t)x * 32 + w];
-    }
+    if (tid < M && (inj.mode & kInjReachesPo))
+      acc[tid] = inj_value(a, inj, w0 + tid) ^ a.good[(uint64_t)x * 32 + w0 + tid];
     __syncthreads();
-    uint64_t pacc[M];
+    PoAcc<M> pacc;
 #pragma unroll
-    for (int m = 0; m < M; ++m) pacc[m] = 0ull;
-    for (uint32_t L = L0; L <= a.max_gate_level; ++L) {
-      const uint32_t lo = a.level_off[L], hi = a.level_off[L + 1];
-      for (uint32_t g = lo + tid; g < hi; g += nth) {
-        const uint32_t mt = a.meta[g];
-        const uint4 fs = a.fslot[g];
-        const uint32_t t = (mt >> kMetaTypeShift) & 15u;
-        const uint32_t nf = ((mt >> kMetaNfShift) & 3u) + 1u;
-        uint64_t i0[M], i1[M], i2[M], i3[M];
-        ld_words<M>(vals + (size_t)fs.x * M, i0);
-        if (nf > 1) ld_words<M>(vals + (size_t)fs.y * M, i1);
-        if (nf > 2) ld_words<M>(vals + (size_t)fs.z * M, i2);
-        if (nf > 3) ld_words<M>(vals + (size_t)fs.w * M, i3);
-        uint64_t r[M];
+    for (int c = 0; c < C; ++c)
 #pragma unroll
-        for (int m = 0; m < M; ++m) r[m] = eval_word(t, nf, i0[m], i1[m], i2[m], i3[m]);
-        if (mt & kMetaHasSlot) st_words<M>(vals + (size_t)(mt & kMetaSlotMask) * M, r);
-        if (mt & kMetaPo) {
-          uint64_t gv[M];
-          ld_words<M>(a.good + (uint64_t)g * 32 + w0, gv);
-#pragma unroll
-          for (int m = 0; m < M; ++m) pacc[m] |= r[m] ^ gv[m];
-        }
+      for (int v = 0; v < VC; ++v) pacc[c][v] = 0ull;
+    bool aborted = false;
+    for (uint32_t L = L0; L <= Lmax; ++L) {
+      const int b = (int)((L - L0) & 1u);
+      const uint32_t nhi = (L < Lmax) ? a.level_off[L + 2] : hi;  // used next level
+      const bool ok = mbar_wait(&bars[b], b ? phase1 : phase0);
+      if (b)
+        phase1 ^= 1u;
+      else
+        phase0 ^= 1u;
+      const uint4* rb = recbuf + (size_t)b * a.rec_buf;
+      for (uint32_t off = my_off; lo + off < hi; off += nth) {
+        const uint4 q = (off < a.rec_buf) ? rb[off] : a.recs[lo + off];
+        gate_dispatch<M>(vals, q, pl, a.good + (uint64_t)q.w * 32 + w0, pacc);
       }
-      __syncthreads();
+      if (__syncthreads_or(!ok)) {
+        aborted = true;
+        break;
+      }
+      if (tid == 0 && L + 2 <= Lmax) stage(L + 2, b);
+      lo = hi;
+      hi = nhi;
+    }
+    if (aborted) {
+      if (tid == 0) atomicExch(a.err, 1);
+      return;
     }
 #pragma unroll
-    for (int m = 0; m < M; ++m)
-      if (pacc[m]) atomicOr(&acc[m], (unsigned long long)pacc[m]);
+    for (int c = 0; c < C; ++c) {
+      const int h = (pl + c) % C;
+#pragma unroll
+      for (int v = 0; v < VC; ++v)
+        if (pacc[c][v]) atomicOr(&acc[VC * h + v], (unsigned long long)pacc[c][v]);
+    }
     __syncthreads();
     if (tid < M) a.out[(uint64_t)si * 32 + w0 + tid] = acc[tid];
   }

@@ -22,12 +22,11 @@ struct GoodArgs {
 };
 
 struct SweepArgs {
-  const uint4* fslot;
-  const uint32_t* meta;
+  const uint4* recs;       // SweepRec per position (see fsimb_plan.h)
   const uint32_t* level;
   const uint32_t* level_off;
   const uint32_t* li_off;
-  const uint32_t* li_elem;
+  const uint32_t* li;      // (element, slot) pairs
   const uint32_t* fi_off;
   const uint32_t* fi_idx;
   const uint8_t* type;
@@ -40,6 +39,9 @@ struct SweepArgs {
   const uint64_t* good;    // this tile: [N][32]
   uint64_t* out;           // this tile: [n_sweeps][32] OR of PO differences
   int* queue;              // work counter for this launch
+  uint32_t vals_bytes;     // shared memory for values (multiple of 16)
+  uint32_t rec_buf;        // records per staging buffer (2 buffers follow the values)
+  int* err;                // set to 1 if a bounded wait gave up
 };
 
 struct FfrArgs {

@@ -5,6 +5,28 @@
 
 namespace fsimb {
 
+namespace {
+
+// Inputs an element's evaluation reads: INV, CLKBUF and PO use their first
+// input only (fsim/simulation.cpp:979-983, 1062-1067, 1074-1077).
+uint32_t eff_fanin(const Netlist& nl, uint32_t e) {
+  uint32_t nf = nl.fanin_count(e);
+  const uint8_t t = nl.type[e];
+  if (t == G_INV || t == G_CLKBUF || t == G_PO) nf = std::min<uint32_t>(nf, 1);
+  return nf;
+}
+
+}  // namespace
+
+uint32_t gate_family(uint8_t t) {
+  switch (t) {
+    case G_XOR:
+    case G_XNOR: return 1;
+    case G_MUX: return 2;
+    default: return 0;
+  }
+}
+
 void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
   P = Plan();
   const uint32_t N = nl.N;
@@ -20,15 +42,17 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     P.max_level_width = std::max<uint32_t>(P.max_level_width, nl.level_off[l + 1] - nl.level_off[l]);
 
   // Per-element fanout facts.
-  std::vector<uint8_t> po_drv(N, 0), gate_fo(N, 0), mux_below(N, 0);
+  std::vector<uint8_t> mux_below(N, 0);
+  P.po_drv.assign(N, 0);
+  P.gate_fo.assign(N, 0);
   P.maxfo_level.assign(N, 0);
   for (uint32_t e = 0; e < N; ++e) {
     for (uint32_t k = nl.fo_off[e]; k < nl.fo_off[e + 1]; ++k) {
       uint32_t c = nl.fo_idx[k];
       if (nl.type[c] == G_PO) {
-        po_drv[e] = 1;
+        P.po_drv[e] = 1;
       } else {
-        gate_fo[e] = 1;
+        P.gate_fo[e] = 1;
         P.maxfo_level[e] = std::max(P.maxfo_level[e], nl.level[c]);
       }
     }
@@ -43,69 +67,20 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     mux_below[e] = hb;
   }
 
-  // Shared-memory slots: interval allocation over live ranges
-  // [level(e), highest consumer level].  Intervals sharing a slot never
-  // overlap, so a slot is rewritten only after its last reader's level.
-  std::vector<uint32_t> slot(N, kNoSlot);
+  // Peak number of live values (interval graph of [level, highest consumer
+  // level]); the schedule may need a few more to honour slot residues.
   {
-    std::vector<std::vector<uint32_t>> release(nl.n_levels + 1);
-    std::vector<uint32_t> free_slots;
-    uint32_t next = 0, live = 0;
+    std::vector<int64_t> delta(nl.n_levels + 2, 0);
+    for (uint32_t e = 0; e < N; ++e)
+      if (P.gate_fo[e]) {
+        delta[nl.level[e]]++;
+        delta[P.maxfo_level[e] + 1]--;
+      }
+    int64_t live = 0;
     for (uint32_t l = 0; l < nl.n_levels; ++l) {
-      for (uint32_t s : release[l]) {
-        free_slots.push_back(s);
-        --live;
-      }
-      for (uint32_t e = nl.level_off[l]; e < nl.level_off[l + 1]; ++e) {
-        if (!gate_fo[e]) continue;
-        uint32_t s;
-        if (!free_slots.empty()) {
-          s = free_slots.back();
-          free_slots.pop_back();
-        } else {
-          s = next++;
-        }
-        slot[e] = s;
-        ++live;
-        release[P.maxfo_level[e] + 1].push_back(s);
-      }
-      P.max_live = std::max(P.max_live, live);
+      live += delta[l];
+      P.max_live = std::max<uint32_t>(P.max_live, (uint32_t)live);
     }
-    P.max_live = std::max(P.max_live, next);
-  }
-
-  // Sweep records.
-  P.fslot.assign((size_t)N * 4, 0);
-  P.meta.assign(N, 0);
-  for (uint32_t e = 0; e < N; ++e) {
-    const uint8_t t = nl.type[e];
-    uint32_t nf = nl.fanin_count(e);
-    // INV, CLKBUF and PO read their first input only (fsim/simulation.cpp:979-983,
-    // 1062-1067, 1074-1077).
-    if (t == G_INV || t == G_CLKBUF || t == G_PO) nf = std::min<uint32_t>(nf, 1);
-    for (uint32_t k = 0; k < nf && k < 4; ++k) P.fslot[(size_t)e * 4 + k] = slot[nl.fi_idx[nl.fi_off[e] + k]];
-    uint32_t m = (slot[e] == kNoSlot ? kNoSlot : slot[e]) & kMetaSlotMask;
-    if (slot[e] != kNoSlot) m |= kMetaHasSlot;
-    if (po_drv[e]) m |= kMetaPo;
-    m |= ((nf ? nf - 1 : 0) & 3u) << kMetaNfShift;
-    m |= ((uint32_t)t & 15u) << kMetaTypeShift;
-    P.meta[e] = m;
-  }
-
-  // Live-in sets: elements whose value a sweep starting at level L reads
-  // before computing it (level(e) < L <= highest consumer level).
-  {
-    std::vector<uint32_t> cnt(nl.n_levels + 2, 0);
-    for (uint32_t e = 0; e < N; ++e)
-      if (slot[e] != kNoSlot)
-        for (uint32_t l = nl.level[e] + 1; l <= P.maxfo_level[e]; ++l) cnt[l]++;
-    P.li_off.assign(nl.n_levels + 1, 0);
-    for (uint32_t l = 0; l < nl.n_levels; ++l) P.li_off[l + 1] = P.li_off[l] + cnt[l];
-    P.li_elem.assign(P.li_off[nl.n_levels], 0);
-    std::vector<uint32_t> fill(P.li_off.begin(), P.li_off.end() - 1);
-    for (uint32_t e = 0; e < N; ++e)
-      if (slot[e] != kNoSlot)
-        for (uint32_t l = nl.level[e] + 1; l <= P.maxfo_level[e]; ++l) P.li_elem[fill[l]++] = e;
   }
 
   // FFR roots.
@@ -117,17 +92,20 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     else
       root[e] = root[nl.fo_idx[nl.fo_off[e]]];
   }
+  auto reaches_po = [&](uint32_t x) {
+    return (nl.type[x] == G_PO || P.po_drv[x]) ? kInjReachesPo : 0u;
+  };
+  auto is_exact = [&](const Fault& ft) {
+    return ft.pin == 0 ? (bool)mux_below[ft.site] : (nl.type[ft.site] == G_MUX || mux_below[ft.site]);
+  };
 
   // Classify faults.
   std::vector<uint32_t> root_id(N, UINT32_MAX);
   std::vector<std::vector<uint32_t>> root_faults;
   std::vector<uint32_t> root_elem;
   for (uint32_t f = 0; f < faults.size(); ++f) {
-    const Fault& ft = faults[f];
-    const uint32_t x = ft.site;
-    bool exact = ft.pin == 0 ? mux_below[x] : (nl.type[x] == G_MUX || mux_below[x]);
-    if (exact) continue;
-    uint32_t r = root[x];
+    if (is_exact(faults[f])) continue;
+    uint32_t r = root[faults[f].site];
     if (root_id[r] == UINT32_MAX) {
       root_id[r] = (uint32_t)root_elem.size();
       root_elem.push_back(r);
@@ -141,7 +119,7 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     uint32_t r = root[e];
     if (r != (uint32_t)e && root_id[r] != UINT32_MAX) root_members[root_id[r]].push_back((uint32_t)e);
   }
-  // Order roots by level so neighbouring warps touch neighbouring data.
+  // Order roots by topological index so neighbouring warps touch neighbouring data.
   std::vector<uint32_t> rorder(root_elem.size());
   for (uint32_t i = 0; i < rorder.size(); ++i) rorder[i] = i;
   std::sort(rorder.begin(), rorder.end(), [&](uint32_t a, uint32_t b) { return root_elem[a] < root_elem[b]; });
@@ -149,13 +127,13 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     const uint32_t r = root_elem[ri];
     RootRec rr{};
     rr.root = r;
-    if (nl.type[r] == G_PO || po_drv[r])
+    if (nl.type[r] == G_PO || P.po_drv[r])
       rr.obs = kObsOne;
-    else if (!gate_fo[r])
+    else if (!P.gate_fo[r])
       rr.obs = kObsZero;
     else {
       rr.obs = (uint32_t)P.sweeps.size();
-      P.sweeps.push_back(InjRec{r, 0, 0, 0});
+      P.sweeps.push_back(InjRec{r, 0, reaches_po(r), 0});
       P.sweep_root.push_back((uint32_t)P.roots.size());
     }
     rr.mem_begin = (uint32_t)P.members.size();
@@ -173,18 +151,16 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
   P.n_stem_sweeps = (uint32_t)P.sweeps.size();
   for (uint32_t f = 0; f < faults.size(); ++f) {
     const Fault& ft = faults[f];
-    const uint32_t x = ft.site;
-    bool exact = ft.pin == 0 ? mux_below[x] : (nl.type[x] == G_MUX || mux_below[x]);
-    if (!exact) continue;
-    P.sweeps.push_back(InjRec{x, ft.pin, 1, ft.value});
+    if (!is_exact(ft)) continue;
+    P.sweeps.push_back(InjRec{ft.site, ft.pin, kInjStuck | reaches_po(ft.site), ft.value});
     P.exact_fault.push_back(f);
   }
+
   // Algorithmic bytes of one gate-word evaluation: its fanin words read and
   // its output word written, 8 * (fanin + 1).
   P.nfp_prefix.assign(N + 1, 0);
   for (uint32_t e = 0; e < N; ++e) {
-    uint32_t nf = ((P.meta[e] >> kMetaNfShift) & 3u) + 1u;
-    if (e < P.n_pi) nf = 0;
+    uint32_t nf = e < P.n_pi ? 0 : eff_fanin(nl, e);
     P.nfp_prefix[e + 1] = P.nfp_prefix[e] + 8ull * (nf + 1);
   }
   const uint32_t gates_end = nl.level_off[std::min(P.max_gate_level + 1, nl.n_levels)];
@@ -195,6 +171,174 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
       P.dense_sweep_bytes += P.nfp_prefix[gates_end] - P.nfp_prefix[nl.level_off[L0]];
     }
   }
+}
+
+// ---------------------------------------------------------------- schedule
+namespace {
+
+struct SlotPool {
+  uint32_t G;
+  uint32_t next_block = 0;
+  std::vector<std::vector<uint32_t>> free;  // per residue
+  explicit SlotPool(uint32_t g) : G(g), free(g) {}
+  uint32_t alloc(uint32_t r) {
+    if (free[r].empty()) {
+      for (uint32_t q = 0; q < G; ++q) free[q].push_back(next_block * G + q);
+      ++next_block;
+    }
+    uint32_t s = free[r].back();
+    free[r].pop_back();
+    return s;
+  }
+  void release(uint32_t s) { free[s % G].push_back(s); }
+};
+
+}  // namespace
+
+void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
+  S = Schedule();
+  S.G = G;
+  const uint32_t N = nl.N;
+  std::vector<uint32_t> slot(N, kNoSlot);
+  SlotPool pool(G);
+  std::vector<std::vector<uint32_t>> release(nl.n_levels + 2);
+  // PIs: residues round robin.
+  uint32_t rr = 0;
+  for (uint32_t e = nl.level_off[0]; e < nl.level_off[1]; ++e) {
+    if (!P.gate_fo[e]) continue;
+    slot[e] = pool.alloc(rr++ % G);
+    release[P.maxfo_level[e] + 1].push_back(slot[e]);
+  }
+  S.recs.assign(N, SweepRec{});
+  auto nf_of = [&](uint32_t e) { return std::min<uint32_t>(eff_fanin(nl, e), 4); };
+  // Classes by (gate family, fan-in): a warp runs one code path.  The AND
+  // family (AND, NAND, OR, NOR, INV, CLKBUF) is io ^ AND(in ^ ii), the XOR
+  // family io ^ XOR(in); MUX is its own family.
+  auto cls_of = [&](uint32_t e) { return gate_family(nl.type[e]) * 8 + nf_of(e); };
+  auto res = [&](uint32_t e, uint32_t k) { return slot[nl.fi_idx[nl.fi_off[e] + k]] % G; };
+  std::vector<uint32_t> order, leftover;
+  // Groups of G consecutive positions inside one class.  Each member is the
+  // candidate adding the fewest repeated residues (per fanin position) to
+  // the group, none if possible; only the last, partial group of a class goes
+  // to a mixed tail at the end of the level.
+  auto make_groups = [&](std::vector<uint32_t>& pool_in, bool tail) {
+    std::vector<uint8_t> taken(pool_in.size(), 0);
+    size_t left = pool_in.size(), first_free = 0;
+    while (left >= G || (tail && left > 0)) {
+      uint32_t used[4] = {0, 0, 0, 0};
+      size_t n_grp = 0;
+      while (n_grp < G && left > 0) {
+        size_t best = SIZE_MAX;
+        int best_cost = 1 << 30;
+        size_t scanned = 0;
+        while (first_free < pool_in.size() && taken[first_free]) ++first_free;
+        for (size_t c = first_free; c < pool_in.size() && scanned < 256; ++c) {
+          if (taken[c]) continue;
+          ++scanned;
+          const uint32_t e = pool_in[c];
+          const uint32_t nf = nf_of(e);
+          int cost = 0;
+          for (uint32_t k = 0; k < nf; ++k) cost += (used[k] >> res(e, k)) & 1u;
+          if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+            if (cost == 0) break;
+          }
+        }
+        if (best == SIZE_MAX) break;  // unreachable: left > 0 leaves a candidate
+        const uint32_t e = pool_in[best];
+        taken[best] = 1;
+        --left;
+        for (uint32_t k = 0; k < nf_of(e); ++k) used[k] |= 1u << res(e, k);
+        order.push_back(e);
+        ++n_grp;
+      }
+    }
+    if (!tail)
+      for (size_t c = 0; c < pool_in.size(); ++c)
+        if (!taken[c]) leftover.push_back(pool_in[c]);
+  };
+  for (uint32_t L = 1; L <= P.max_gate_level && L < nl.n_levels; ++L) {
+    for (uint32_t s : release[L]) pool.release(s);
+    const uint32_t lo = nl.level_off[L], hi = nl.level_off[L + 1];
+    std::vector<uint32_t> elems(hi - lo);
+    for (uint32_t i = 0; i < hi - lo; ++i) elems[i] = lo + i;
+    std::stable_sort(elems.begin(), elems.end(),
+                     [&](uint32_t a, uint32_t b) { return cls_of(a) < cls_of(b); });
+    order.clear();
+    leftover.clear();
+    for (size_t i = 0; i < elems.size();) {
+      size_t j = i;
+      while (j < elems.size() && cls_of(elems[j]) == cls_of(elems[i])) ++j;
+      std::vector<uint32_t> cls(elems.begin() + i, elems.begin() + j);
+      make_groups(cls, false);
+      i = j;
+    }
+    std::stable_sort(leftover.begin(), leftover.end(),
+                     [&](uint32_t a, uint32_t b) { return cls_of(a) < cls_of(b); });
+    make_groups(leftover, true);
+    // Positions, output slots (residue = position mod G) and records.
+    for (uint32_t o = 0; o < order.size(); ++o) {
+      const uint32_t e = order[o];
+      SweepRec r{};
+      const uint32_t nf = nf_of(e);
+      for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)slot[nl.fi_idx[nl.fi_off[e] + k]];
+      uint32_t meta = (uint32_t)nl.type[e] & kRecTypeMask;
+      meta |= ((nf ? nf - 1 : 0) & 3u) << kRecNfShift;
+      if (P.po_drv[e]) meta |= kRecPo;
+      if (P.gate_fo[e]) {
+        slot[e] = pool.alloc(o % G);
+        release[P.maxfo_level[e] + 1].push_back(slot[e]);
+        meta |= kRecHasSlot;
+        r.slot = (uint16_t)slot[e];
+      }
+      r.meta = (uint16_t)meta;
+      r.elem = e;
+      S.recs[lo + o] = r;
+    }
+    // Bank-conflict accounting per aligned group of G positions.
+    for (uint32_t g0 = 0; g0 < order.size(); g0 += G) {
+      const uint32_t g1 = std::min<uint32_t>(g0 + G, (uint32_t)order.size());
+      for (uint32_t k = 0; k < 5; ++k) {
+        uint32_t seen = 0, any = 0;
+        bool conflict = false;
+        for (uint32_t o = g0; o < g1; ++o) {
+          const SweepRec& r = S.recs[lo + o];
+          uint32_t s;
+          if (k < 4) {
+            if (k >= ((r.meta >> kRecNfShift) & 3u) + 1u) continue;
+            s = r.fs[k];
+          } else {
+            if (!(r.meta & kRecHasSlot)) continue;
+            s = r.slot;
+          }
+          any = 1;
+          conflict |= (seen >> (s % G)) & 1u;
+          seen |= 1u << (s % G);
+        }
+        S.access_groups += any;
+        S.conflict_groups += conflict;
+      }
+    }
+  }
+  S.max_live = pool.next_block * G;
+  if (S.max_live > kMaxSlots) return;
+  // Live-in sets as (element, slot) pairs.
+  std::vector<uint32_t> cnt(nl.n_levels + 2, 0);
+  for (uint32_t e = 0; e < N; ++e)
+    if (slot[e] != kNoSlot)
+      for (uint32_t l = nl.level[e] + 1; l <= P.maxfo_level[e]; ++l) cnt[l]++;
+  S.li_off.assign(nl.n_levels + 1, 0);
+  for (uint32_t l = 0; l < nl.n_levels; ++l) S.li_off[l + 1] = S.li_off[l] + cnt[l];
+  S.li.assign(2ull * S.li_off[nl.n_levels], 0);
+  std::vector<uint32_t> fill(S.li_off.begin(), S.li_off.end() - 1);
+  for (uint32_t e = 0; e < N; ++e)
+    if (slot[e] != kNoSlot)
+      for (uint32_t l = nl.level[e] + 1; l <= P.maxfo_level[e]; ++l) {
+        const uint32_t i = fill[l]++;
+        S.li[2 * i] = e;
+        S.li[2 * i + 1] = slot[e];
+      }
 }
 
 }  // namespace fsimb

@@ -4,10 +4,16 @@
 // Layout in HBM (all arrays indexed by the reference's topological index):
 //   type[N]            u8 gate type
 //   fi_off[N+1], fi_idx[E]   fanin CSR in pin order (good-machine kernel)
-//   sw_fslot[N]        uint4: shared-memory slot of each of up to 4 fanins
-//   sw_meta[N]         u32: own slot | has_slot | drives_po | nfanin-1 | type
-//   li_off[L+1], li_elem[]   elements whose value is live when a sweep starts
-//                            at level L (read from the good values at start)
+//   sweep_rec[N]       16-byte record per position of the sweep order: the
+//                      shared-memory slots of up to 4 fanins, the own slot,
+//                      type / fan-in / flags and the element index.  Within a
+//                      level the order is by gate class (family, fan-in), and
+//                      every group of G consecutive positions has pairwise
+//                      different slot residues mod G for each fanin and for
+//                      the output wherever the host found such groups, so the
+//                      group's shared-memory accesses hit distinct banks
+//   li_off[L+1], li[]  (element, slot) pairs live when a sweep starts at
+//                      level L (read from the good values at start)
 //   good[tile][N][32]  u64 good-machine words, 32 words (2048 patterns) per tile
 //
 // Fault handling:
@@ -30,18 +36,30 @@
 namespace fsimb {
 
 constexpr uint32_t kTileWords = 32;  // words per tile = lanes of a warp
-constexpr uint32_t kNoSlot = 0x7FFFFFu;
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+constexpr uint32_t kMaxSlots = 65535;   // slots are 16-bit in the sweep records
 
-// sw_meta bit fields
-constexpr uint32_t kMetaSlotMask = 0x7FFFFFu;
-constexpr uint32_t kMetaHasSlot = 1u << 23;
-constexpr uint32_t kMetaPo = 1u << 24;
-constexpr int kMetaNfShift = 25;   // 2 bits: nfanin - 1
-constexpr int kMetaTypeShift = 27; // 4 bits
+// SweepRec::meta bit fields
+constexpr uint32_t kRecTypeMask = 15u;     // bits 0-3: gate type
+constexpr int kRecNfShift = 4;             // bits 4-5: fan-in - 1
+constexpr uint32_t kRecPo = 1u << 6;       // drives a PO
+constexpr uint32_t kRecHasSlot = 1u << 7;  // has gate consumers (value stored)
+
+// InjRec::mode bit fields
+constexpr uint32_t kInjStuck = 1u;      // 0: flip the element's word, 1: stuck value
+constexpr uint32_t kInjReachesPo = 2u;  // the element is, or drives, a PO
 
 // Observability source of an FFR root.
 constexpr uint32_t kObsZero = 0xFFFFFFFEu;  // root reaches no PO
 constexpr uint32_t kObsOne = 0xFFFFFFFFu;   // root is / drives a PO
+
+struct SweepRec {
+  uint16_t fs[4];  // fanin slots
+  uint16_t slot;   // own slot (valid with kRecHasSlot)
+  uint16_t meta;
+  uint32_t elem;   // topological index
+};
+static_assert(sizeof(SweepRec) == 16, "SweepRec is one 16-byte load");
 
 struct RootRec {
   uint32_t root;
@@ -70,7 +88,7 @@ struct TracedRec {  // one traced fault
 struct InjRec {     // sweep injection: flip (stem) or stuck (exact fault)
   uint32_t elem;
   uint32_t pin;     // exact faults: 0 output, k input; flips: 0
-  uint32_t mode;    // 0 flip, 1 stuck
+  uint32_t mode;    // kInjStuck | kInjReachesPo
   uint32_t value;
 };
 
@@ -78,17 +96,15 @@ struct Plan {
   uint32_t N = 0, n_pi = 0, n_gates = 0, n_po = 0;
   uint32_t n_levels = 0;
   uint32_t max_gate_level = 0;       // highest level holding a non-PO element
-  uint32_t max_live = 0;             // shared-memory slots needed by a sweep
+  uint32_t max_live = 0;             // slots needed without residue constraints
   uint32_t max_level_width = 0;
   uint64_t dense_sweep_gates = 0;    // sum over sweeps of gates evaluated
   uint64_t dense_sweep_bytes = 0;    // sum over sweeps of 8*(fanin+1) per evaluated gate, per word
   std::vector<uint64_t> nfp_prefix;  // [N+1] prefix sums of 8*(effective fanin+1)
   std::vector<uint32_t> level_off;   // [n_levels+1]
-  std::vector<uint32_t> fslot;       // [4N]
-  std::vector<uint32_t> meta;        // [N]
-  std::vector<uint32_t> li_off;      // [n_levels+1]
-  std::vector<uint32_t> li_elem;
   std::vector<uint32_t> maxfo_level; // [N] highest non-PO consumer level (0 if none)
+  std::vector<uint8_t> gate_fo;      // [N] has a non-PO consumer
+  std::vector<uint8_t> po_drv;       // [N] drives a PO
   // traced faults
   std::vector<RootRec> roots;
   std::vector<MemberRec> members;
@@ -101,6 +117,23 @@ struct Plan {
   bool has_mux = false;
 };
 
+// Per-level evaluation order and shared-memory slots for one residue group
+// size G (16 / words per item).
+struct Schedule {
+  uint32_t G = 0;
+  uint32_t max_live = 0;             // slots (multiple of G)
+  std::vector<SweepRec> recs;        // [N], positions of levels 1..max_gate_level used
+  std::vector<uint32_t> li_off;      // [n_levels+1]
+  std::vector<uint32_t> li;          // pairs (element, slot)
+  uint64_t conflict_groups = 0;      // group accesses whose slots repeat a residue
+  uint64_t access_groups = 0;        // group accesses (fanin loads + stores)
+};
+
+// 0: AND family (AND, NAND, OR, NOR, INV, CLKBUF, PO), 1: XOR family, 2: MUX.
+uint32_t gate_family(uint8_t type);
 void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& plan);
+// G in {2, 4, 8, 16}.  A schedule that needs more than kMaxSlots slots
+// reports max_live > kMaxSlots and leaves li empty.
+void build_schedule(const Netlist& nl, const Plan& plan, uint32_t G, Schedule& out);
 
 }  // namespace fsimb
