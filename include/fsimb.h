@@ -148,6 +148,11 @@ int fsimb_types(const fsimb_handle* h, uint8_t* out, uint64_t n);
 int fsimb_faults(const fsimb_handle* h, uint32_t* site, uint8_t* pin, uint8_t* value, uint64_t n);
 /* loaded pattern words, n = rounds * nPI */
 int fsimb_patterns(const fsimb_handle* h, uint64_t* out, uint64_t n);
+/* Graphviz DOT text of the loaded circuit in the layout of the reference's
+ * Simulator::visualization_graph (fsim/simulation.cpp:1157-1236): fanin
+ * edges of gates and POs inside cluster_0, then the PI and PO nodes.
+ * Works on host-only handles.  Release the text with fsimb_free_text. */
+int fsimb_dot(const fsimb_handle* h, char** text, size_t* len);
 
 /* Good-machine PO words without allocating device memory.  This entry point
  * has no counterpart in the reference.  It serves callers that may not call

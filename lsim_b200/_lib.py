@@ -107,6 +107,7 @@ SIGNATURES = {
     "fsimb_gen_patterns": (ctypes.c_int, [_U64, _U64, _U64, ctypes.c_double, ctypes.c_double,
                                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ)]),
     "fsimb_free_text": (None, [ctypes.c_void_p]),
+    "fsimb_dot": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ)]),
     "fsimb_good_po_noalloc": (ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                              ctypes.c_void_p]),
 }

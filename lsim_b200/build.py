@@ -18,8 +18,10 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 CXX_SOURCES = ["fsimb_netlist.cpp", "fsimb_gen.cpp", "fsimb_plan.cpp"]
 CU_SOURCES = ["fsimb_kernels.cu", "fsimb_engine.cu"]
-HEADERS = ["fsimb_netlist.h", "fsimb_gen.h", "fsimb_plan.h", "fsimb_kernels.cuh"]
+HEADERS = ["fsimb_netlist.h", "fsimb_gen.h", "fsimb_plan.h", "fsimb_kernels.cuh", "fsimb_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+APPS = ["fsimb_simple", "fsimb_ma_partition"]  # drop-ins for main/simple and MA_cuda_partition
+BIN = os.path.join(HERE, "bin")
 
 
 def _nvcc():
@@ -73,6 +75,16 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)
+    os.makedirs(BIN, exist_ok=True)
+    for app in APPS:
+        s = os.path.join(CSRC, "apps", app + ".cpp")
+        exe = os.path.join(BIN, app)
+        if force or _stale(exe, [s, LIB, os.path.join(INCLUDE, "fsimb.h")]):
+            cmd = [cxx, "-std=c++17", "-O2", "-I" + INCLUDE, s, "-o", exe, "-L" + HERE,
+                   "-lfsimb200", "-Wl,-rpath,$ORIGIN/.."]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
     return LIB
 
 

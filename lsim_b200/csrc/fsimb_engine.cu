@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -21,72 +22,23 @@
 
 #include "../../include/fsimb.h"
 #include "fsimb_gen.h"
+#include "fsimb_internal.h"
 #include "fsimb_kernels.cuh"
 #include "fsimb_netlist.h"
 #include "fsimb_plan.h"
 
 using namespace fsimb;
 
+namespace fsimb {
+uint64_t next_generation() {
+  static std::atomic<uint64_t> g{0};
+  return ++g;
+}
+}  // namespace fsimb
+
 namespace {
 
 thread_local std::string g_create_error;
-
-struct CudaError {
-  std::string msg;
-};
-struct LimitError {
-  std::string msg;
-};
-struct StateError {
-  std::string msg;
-};
-struct ArgError {
-  std::string msg;
-};
-struct IoError {
-  std::string msg;
-};
-
-#define CK(call)                                                                          \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_)};                \
-  } while (0)
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t n = 0;
-  void ensure(size_t bytes) {
-    if (bytes <= n && p) return;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      cudaGetLastError();
-      throw CudaError{"cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
-    }
-    n = bytes;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  template <class T>
-  T* as() const {
-    return reinterpret_cast<T*>(p);
-  }
-};
-
-template <class T>
-void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
-  b.ensure(v.size() * sizeof(T));
-  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-}
 
 std::string read_file(const char* path) {
   std::ifstream f(path, std::ios::binary);
@@ -97,118 +49,6 @@ std::string read_file(const char* path) {
 }
 
 }  // namespace
-
-struct fsimb_handle {
-  int device = -1;
-  int n_sms = 0;
-  size_t smem_optin = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-
-  Netlist nl;
-  bool has_ckt = false;
-  std::vector<Fault> faults;
-  bool has_faults = false;
-  Patterns pats;
-  bool has_pats = false;
-
-  Plan plan;
-  bool plan_valid = false;
-  bool plan_uploaded = false;
-  Schedule sched;          // for sched_M words per item
-  int sched_M = 0;
-  bool sched_uploaded = false;
-
-  DevBuf d_type, d_fi_off, d_fi_idx, d_recs, d_level, d_level_off, d_li_off, d_li;
-  DevBuf d_roots, d_members, d_traced, d_inj, d_exact;
-  DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue, d_err;
-  DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout;
-  uint64_t good_tiles = 0;  // tiles held in d_good
-  uint64_t good_P = 0;
-  bool pats_uploaded = false;  // d_pwords holds the current patterns
-
-  std::vector<fsimb_fault_result> results;
-  bool has_results = false;
-  fsimb_stats stats{};
-  std::vector<cudaEvent_t> events;
-
-  ~fsimb_handle() {
-    if (device >= 0) {
-      cudaSetDevice(device);
-      for (DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
-                        &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
-                        &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
-                        &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
-                        &d_exact_list[0], &d_exact_list[1], &d_nout})
-        b->release();
-      for (auto e : events) cudaEventDestroy(e);
-      if (stream) cudaStreamDestroy(stream);
-    }
-  }
-
-  cudaEvent_t ev(size_t i) {
-    while (events.size() <= i) {
-      cudaEvent_t e;
-      CK(cudaEventCreate(&e));
-      events.push_back(e);
-    }
-    return events[i];
-  }
-
-  uint64_t device_bytes() const {
-    uint64_t s = 0;
-    for (const DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
-                            &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
-                            &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
-                            &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
-                            &d_exact_list[0], &d_exact_list[1], &d_nout})
-      s += b->n;
-    return s;
-  }
-
-  void invalidate_circuit() {
-    has_faults = false;
-    has_pats = false;
-    plan_valid = false;
-    plan_uploaded = false;
-    sched_M = 0;
-    sched_uploaded = false;
-    has_results = false;
-    good_tiles = 0;
-  }
-
-  void load_ckt(const char* t, size_t n) {
-    Netlist tmp;
-    parse_ckt(t, n, tmp);
-    nl = std::move(tmp);
-    has_ckt = true;
-    invalidate_circuit();
-    faults.clear();
-    pats = Patterns();
-  }
-  void load_flst(const char* t, size_t n) {
-    if (!has_ckt) throw StateError{"load a circuit first"};
-    std::vector<Fault> tmp;
-    parse_flst(t, n, nl, tmp);
-    faults = std::move(tmp);
-    has_faults = true;
-    plan_valid = false;
-    plan_uploaded = false;
-    has_results = false;
-  }
-  void load_ptn(const char* t, size_t n) {
-    if (!has_ckt) throw StateError{"load a circuit first"};
-    Patterns tmp;
-    parse_ptn(t, n, nl, tmp);
-    pats = std::move(tmp);
-    has_pats = true;
-    has_results = false;
-    good_tiles = 0;
-    pats_uploaded = false;
-  }
-
-  void run(const fsimb_opts* opts);
-};
 
 // --------------------------------------------------------------------------
 void fsimb_handle::run(const fsimb_opts* opts) {
@@ -281,31 +121,8 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   }
   const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (budget - vals_bytes) / 32);
   const size_t smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
-  // CTA size: one thread per gate of a level; the multiple of 32 that splits
-  // the typical (90th percentile) level width into equal rounds, so no
-  // thread idles long before the per-level barrier.
-  const uint32_t tmax = M >= 8 ? 512 : (M >= 4 ? 768 : 1024);
-  int threads = (int)o.block_threads;
-  if (!threads) {
-    uint32_t w = 64;
-    if (!widths.empty()) {
-      std::nth_element(widths.begin(), widths.begin() + widths.size() * 9 / 10, widths.end());
-      w = std::max<uint32_t>(widths[widths.size() * 9 / 10], 1);
-    }
-    uint32_t best = 64;
-    double best_cost = 1e30;
-    for (uint32_t k = 1; k <= 64; ++k) {
-      uint32_t t = (w + k - 1) / k;
-      t = std::max<uint32_t>(64, (t + 31) / 32 * 32);
-      if (t > tmax) continue;
-      const double cost = (double)k * t + 8.0 * k;  // issued slots + per-round overhead
-      if (cost < best_cost) {
-        best_cost = cost;
-        best = t;
-      }
-    }
-    threads = (int)best;
-  }
+  const uint32_t tmax = sweep_max_threads(M);
+  int threads = o.block_threads ? (int)o.block_threads : (int)pick_sweep_threads(widths, M);
   threads = std::min<int>(threads, (int)tmax);
 
   cudaEvent_t e0 = ev(0), e1 = ev(1), e2 = ev(2), e3 = ev(3);
@@ -599,47 +416,6 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   stats.device_bytes = device_bytes();
 }
 
-// -------------------------------------------------------------------- C ABI
-#define API_BEGIN(h)                                 \
-  if (!(h)) return FSIMB_ERR_ARG;                    \
-  try {
-#define API_END(h)                                   \
-  }                                                  \
-  catch (const ParseError& e) {                      \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_PARSE;                          \
-  }                                                  \
-  catch (const CudaError& e) {                       \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_CUDA;                           \
-  }                                                  \
-  catch (const LimitError& e) {                      \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_LIMIT;                          \
-  }                                                  \
-  catch (const StateError& e) {                      \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_STATE;                          \
-  }                                                  \
-  catch (const ArgError& e) {                        \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_ARG;                            \
-  }                                                  \
-  catch (const IoError& e) {                         \
-    (h)->err = e.msg;                                \
-    return FSIMB_ERR_IO;                             \
-  }                                                  \
-  catch (const std::bad_alloc&) {                    \
-    (h)->err = "host allocation failed";             \
-    return FSIMB_ERR_NOMEM;                          \
-  }                                                  \
-  catch (const std::exception& e) {                  \
-    (h)->err = e.what();                             \
-    return FSIMB_ERR_ARG;                            \
-  }                                                  \
-  (h)->err.clear();                                  \
-  return FSIMB_OK;
-
 extern "C" {
 
 int fsimb_create(int device, fsimb_handle** out) {
@@ -734,6 +510,7 @@ int fsimb_set_faults(fsimb_handle* h, const uint32_t* site, const uint8_t* pin,
   }
   h->faults = std::move(fs);
   h->has_faults = true;
+  h->gen = next_generation();
   h->plan_valid = false;
   h->plan_uploaded = false;
   h->has_results = false;
@@ -759,6 +536,7 @@ int fsimb_set_patterns(fsimb_handle* h, const uint64_t* words, uint64_t num_patt
   p.words.assign(words, words + W * h->nl.n_pi);
   h->pats = std::move(p);
   h->has_pats = true;
+  h->gen = next_generation();
   h->has_results = false;
   h->good_tiles = 0;
   h->pats_uploaded = false;
@@ -901,6 +679,43 @@ static int emit_text(const std::string& s, char** text, size_t* len) {
   *text = p;
   if (len) *len = s.size();
   return FSIMB_OK;
+}
+
+static const char* type_name(uint8_t t) {
+  static const char* names[] = {"INV", "AND", "OR", "XOR", "NAND", "NOR", "XNOR", "MUX", "CLKBUF", "PI", "PO"};
+  return t <= G_PO ? names[t] : "UNKNOWN";
+}
+
+int fsimb_dot(const fsimb_handle* hc, char** text, size_t* len) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!text) throw ArgError{"null output"};
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  const Netlist& nl = h->nl;
+  const uint64_t g0 = nl.n_pi, p0 = nl.n_pi + nl.n_gates;
+  // Node names: PI_i, Gate_j_TYPE (j = index among gates), PO_k.
+  auto src_name = [&](uint32_t e) {
+    if (nl.type[e] == G_PI) return "PI_" + std::to_string(e);
+    return "Gate_" + std::to_string(e - g0) + "_" + type_name(nl.type[e]);
+  };
+  std::string out = "digraph G {\n\tsubgraph cluster_0 {\n\t\tcolor=black;\n"
+                    "\t\tnode [style=filled,color=lightgrey];\n";
+  for (uint64_t e = g0; e < nl.N; ++e) {
+    const std::string dst = e < p0 ? "Gate_" + std::to_string(e - g0) + "_" + type_name(nl.type[e]) + ";"
+                                   : "PO_" + std::to_string(e - p0) + ";";
+    for (uint32_t k = nl.fi_off[e]; k < nl.fi_off[e + 1]; ++k)
+      out += "\t\t" + src_name(nl.fi_idx[k]) + " -> " + dst + "\n";
+  }
+  out += "\t}\n\n";
+  for (uint64_t i = 0; i < nl.n_pi; ++i) out += "\tPI_" + std::to_string(i) + "  [shape=Msquare];\n";
+  for (uint64_t i = 0; i < nl.n_po; ++i) out += "\tPO_" + std::to_string(i) + "  [shape=Msquare];\n";
+  out += "}\n\n";
+  char* p = (char*)std::malloc(out.size() + 1);
+  if (!p) throw std::bad_alloc();
+  std::memcpy(p, out.data(), out.size() + 1);
+  *text = p;
+  if (len) *len = out.size();
+  API_END(h)
 }
 
 int fsimb_gen_circuit(const fsimb_gen_config* cfg, char** text, size_t* len) {

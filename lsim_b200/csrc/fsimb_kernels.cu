@@ -23,6 +23,8 @@
 // rd*64 + bits-1-b.
 #include "fsimb_kernels.cuh"
 
+#include <algorithm>
+
 namespace fsimb {
 
 namespace {
@@ -127,9 +129,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// Index of the last prefix entry <= x (prefix[0] = 0, n entries).
+__device__ __forceinline__ uint32_t find_prefix(const unsigned long long* prefix, uint32_t n,
+                                                unsigned long long x) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (prefix[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 // ---------------------------------------------------------------- sweep
+// Per-circuit pointers a sweep item reads (one circuit, one tile).
+struct SweepView {
+  const uint4* recs;
+  const uint32_t* level;
+  const uint32_t* level_off;
+  const uint32_t* li_off;
+  const uint32_t* li;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const uint64_t* good;  // tile [N][32]
+  uint32_t max_gate_level;
+};
+
 // Faulty value of the injection element for word w of the tile.
-__device__ __forceinline__ uint64_t inj_value(const SweepArgs& a, const InjRec& inj, uint32_t w) {
+__device__ __forceinline__ uint64_t inj_value(const SweepView& a, const InjRec& inj, uint32_t w) {
   const uint32_t x = inj.elem;
   if (!(inj.mode & kInjStuck)) return ~a.good[(uint64_t)x * 32 + w];
   const uint64_t sv = inj.value ? ~0ull : 0ull;
@@ -279,125 +306,197 @@ __device__ __forceinline__ void gate_dispatch(uint64_t* vals, const uint4 q, int
 // Gate records are staged per level into two shared-memory buffers by TMA
 // bulk copies issued two levels ahead (one elected thread, mbarrier
 // completion); a level wider than a buffer reads the rest from global.
+struct SweepCta {
+  uint64_t* vals;     // [max_live][M]
+  uint4* recbuf;      // [2][rec_buf]
+  uint64_t* bars;     // [2] mbarriers
+  unsigned long long* acc;
+  uint32_t rec_buf;
+  uint32_t phase0, phase1;
+};
+
 template <int M>
-__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(SweepArgs a) {
-  constexpr int C = (M >= 2) ? M / 2 : 1;   // chunks per slot
-  constexpr int VC = (M >= 2) ? 2 : 1;      // words per chunk
-  constexpr int G = 16 / M;                 // residue group size
-  constexpr int PH = (M == 1) ? 16 : 8;     // lanes per shared-memory phase
-  extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M] | recbuf[2][rec_buf]
-  __shared__ unsigned long long acc[M];
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ int s_item;
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int pl = tid & (PH - 1);
-  const uint32_t my_off = (uint32_t)((tid & ~(PH - 1)) + ((M >= 2) ? (pl % C) * G + pl / C : pl));
-  const uint32_t n_items = a.n_list * a.subtiles;
-  const uint32_t Lmax = a.max_gate_level;
-  uint4* recbuf = reinterpret_cast<uint4*>(reinterpret_cast<char*>(vals) + a.vals_bytes);
+__device__ __forceinline__ void sweep_cta_init(SweepCta& k, uint64_t* vals, uint32_t vals_bytes,
+                                               uint32_t rec_buf, uint64_t* bars, unsigned long long* acc) {
+  k.vals = vals;
+  k.recbuf = reinterpret_cast<uint4*>(reinterpret_cast<char*>(vals) + vals_bytes);
+  k.bars = bars;
+  k.acc = acc;
+  k.rec_buf = rec_buf;
+  k.phase0 = k.phase1 = 0;
   // Zeroed buffers: a record read before its copy landed names slot 0 and
   // element 0, both in range.
-  for (uint32_t i = tid; i < 2 * a.rec_buf; i += nth) recbuf[i] = make_uint4(0, 0, 0, 0);
-  if (tid == 0) {
+  for (uint32_t i = threadIdx.x; i < 2 * rec_buf; i += blockDim.x) k.recbuf[i] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  uint32_t phase0 = 0, phase1 = 0;
-  auto stage = [&](uint32_t L, int b) {  // thread 0 only
-    const uint32_t lo = a.level_off[L], hi = a.level_off[L + 1];
-    const uint32_t n = min(hi - lo, a.rec_buf);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    bulk_load(recbuf + (size_t)b * a.rec_buf, a.recs + lo, n * 16u, &bars[b]);
-  };
+}
+
+__device__ __forceinline__ void sweep_stage(SweepCta& k, const SweepView& v, uint32_t L, int b) {
+  const uint32_t lo = v.level_off[L], hi = v.level_off[L + 1];
+  const uint32_t n = min(hi - lo, k.rec_buf);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  bulk_load(k.recbuf + (size_t)b * k.rec_buf, v.recs + lo, n * 16u, &k.bars[b]);
+}
+
+// One item: the levels above the injection element for M words starting at
+// word w0 of the tile; writes the OR of PO differences to out_row[w0..w0+M).
+// Returns false (on every thread) if a bounded wait gave up.
+template <int M>
+__device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, const InjRec inj, uint32_t w0,
+                                           uint64_t* out_row) {
+  constexpr int C = (M >= 2) ? M / 2 : 1;   // chunks per slot
+  constexpr int VC = (M >= 2) ? 2 : 1;      // words per chunk
+  constexpr int G = 16 / M;                 // residue group size
+  constexpr int PH = (M == 1) ? 16 : 8;     // lanes per shared-memory phase
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int pl = tid & (PH - 1);
+  const uint32_t my_off = (uint32_t)((tid & ~(PH - 1)) + ((M >= 2) ? (pl % C) * G + pl / C : pl));
+  const uint32_t Lmax = v.max_gate_level;
+  uint64_t* vals = k.vals;
+  const uint32_t x = inj.elem;
+  const uint32_t L0 = v.level[x] + 1;
+  if (tid < M) k.acc[tid] = 0ull;
+  if (tid == 0 && L0 <= Lmax) {
+    sweep_stage(k, v, L0, 0);
+    if (L0 + 1 <= Lmax) sweep_stage(k, v, L0 + 1, 1);
+  }
+  uint32_t lo = 0, hi = 0;
+  if (L0 <= Lmax) {
+    lo = v.level_off[L0];
+    hi = v.level_off[L0 + 1];
+    // Values live at the start level come from the good machine, except
+    // the injection element itself.
+    const uint32_t i1 = v.li_off[L0 + 1];
+    for (uint32_t i = v.li_off[L0] + tid; i < i1; i += nth) {
+      const uint2 es = reinterpret_cast<const uint2*>(v.li)[i];
+      uint64_t* dst = vals + (size_t)es.y * M;
+      if (es.x == x) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) dst[m] = inj_value(v, inj, w0 + m);
+      } else {
+        const uint64_t* src = v.good + (uint64_t)es.x * 32 + w0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) dst[m] = src[m];
+      }
+    }
+  }
+  if (tid < M && (inj.mode & kInjReachesPo))
+    k.acc[tid] = inj_value(v, inj, w0 + tid) ^ v.good[(uint64_t)x * 32 + w0 + tid];
+  __syncthreads();
+  PoAcc<M> pacc;
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+#pragma unroll
+    for (int q = 0; q < VC; ++q) pacc[c][q] = 0ull;
+  for (uint32_t L = L0; L <= Lmax; ++L) {
+    const int b = (int)((L - L0) & 1u);
+    const uint32_t nhi = (L < Lmax) ? v.level_off[L + 2] : hi;  // used next level
+    const bool ok = mbar_wait(&k.bars[b], b ? k.phase1 : k.phase0);
+    if (b)
+      k.phase1 ^= 1u;
+    else
+      k.phase0 ^= 1u;
+    const uint4* rb = k.recbuf + (size_t)b * k.rec_buf;
+    for (uint32_t off = my_off; lo + off < hi; off += nth) {
+      const uint4 q = (off < k.rec_buf) ? rb[off] : v.recs[lo + off];
+      gate_dispatch<M>(vals, q, pl, v.good + (uint64_t)q.w * 32 + w0, pacc);
+    }
+    if (__syncthreads_or(!ok)) return false;
+    if (tid == 0 && L + 2 <= Lmax) sweep_stage(k, v, L + 2, b);
+    lo = hi;
+    hi = nhi;
+  }
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int h = (pl + c) % C;
+#pragma unroll
+    for (int q = 0; q < VC; ++q)
+      if (pacc[c][q]) atomicOr(&k.acc[VC * h + q], (unsigned long long)pacc[c][q]);
+  }
+  __syncthreads();
+  if (tid < M) out_row[w0 + tid] = k.acc[tid];
+  return true;
+}
+
+template <int M>
+__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(SweepArgs a) {
+  extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M] | recbuf[2][rec_buf]
+  __shared__ unsigned long long acc[M];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int s_item;
+  SweepCta k;
+  sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc);
+  const SweepView v{a.recs, a.level, a.level_off, a.li_off, a.li, a.fi_off, a.fi_idx, a.type, a.good,
+                    a.max_gate_level};
+  const uint32_t n_items = a.n_list * a.subtiles;
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(a.queue, 1);
-    if (tid < M) acc[tid] = 0ull;
+    if (threadIdx.x == 0) s_item = atomicAdd(a.queue, 1);
     __syncthreads();
     const uint32_t item = (uint32_t)s_item;
+    __syncthreads();  // s_item is rewritten for the next item only after all have read it
     if (item >= n_items) return;
     const uint32_t li = item / a.subtiles;
     const uint32_t w0 = (item % a.subtiles) * M;
     const uint32_t si = a.list ? a.list[li] : li;
-    const InjRec inj = a.inj[si];
-    const uint32_t x = inj.elem;
-    const uint32_t L0 = a.level[x] + 1;
-    if (tid == 0 && L0 <= Lmax) {
-      stage(L0, 0);
-      if (L0 + 1 <= Lmax) stage(L0 + 1, 1);
-    }
-    uint32_t lo = 0, hi = 0;
-    if (L0 <= Lmax) {
-      lo = a.level_off[L0];
-      hi = a.level_off[L0 + 1];
-      // Values live at the start level come from the good machine, except
-      // the injection element itself.
-      const uint32_t i1 = a.li_off[L0 + 1];
-      for (uint32_t i = a.li_off[L0] + tid; i < i1; i += nth) {
-        const uint2 es = reinterpret_cast<const uint2*>(a.li)[i];
-        uint64_t* dst = vals + (size_t)es.y * M;
-        if (es.x == x) {
-#pragma unroll
-          for (int m = 0; m < M; ++m) dst[m] = inj_value(a, inj, w0 + m);
-        } else {
-          const uint64_t* src = a.good + (uint64_t)es.x * 32 + w0;
-#pragma unroll
-          for (int m = 0; m < M; ++m) dst[m] = src[m];
-        }
-      }
-    }
-    if (tid < M && (inj.mode & kInjReachesPo))
-      acc[tid] = inj_value(a, inj, w0 + tid) ^ a.good[(uint64_t)x * 32 + w0 + tid];
-    __syncthreads();
-    PoAcc<M> pacc;
-#pragma unroll
-    for (int c = 0; c < C; ++c)
-#pragma unroll
-      for (int v = 0; v < VC; ++v) pacc[c][v] = 0ull;
-    bool aborted = false;
-    for (uint32_t L = L0; L <= Lmax; ++L) {
-      const int b = (int)((L - L0) & 1u);
-      const uint32_t nhi = (L < Lmax) ? a.level_off[L + 2] : hi;  // used next level
-      const bool ok = mbar_wait(&bars[b], b ? phase1 : phase0);
-      if (b)
-        phase1 ^= 1u;
-      else
-        phase0 ^= 1u;
-      const uint4* rb = recbuf + (size_t)b * a.rec_buf;
-      for (uint32_t off = my_off; lo + off < hi; off += nth) {
-        const uint4 q = (off < a.rec_buf) ? rb[off] : a.recs[lo + off];
-        gate_dispatch<M>(vals, q, pl, a.good + (uint64_t)q.w * 32 + w0, pacc);
-      }
-      if (__syncthreads_or(!ok)) {
-        aborted = true;
-        break;
-      }
-      if (tid == 0 && L + 2 <= Lmax) stage(L + 2, b);
-      lo = hi;
-      hi = nhi;
-    }
-    if (aborted) {
-      if (tid == 0) atomicExch(a.err, 1);
+    if (!sweep_item<M>(k, v, a.inj[si], w0, a.out + (uint64_t)si * 32)) {
+      if (threadIdx.x == 0) atomicExch(a.err, 1);
       return;
     }
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const int h = (pl + c) % C;
-#pragma unroll
-      for (int v = 0; v < VC; ++v)
-        if (pacc[c][v]) atomicOr(&acc[VC * h + v], (unsigned long long)pacc[c][v]);
+  }
+}
+
+// Batch form: items of many circuits of one shape class, in circuit order;
+// each item names (circuit, tile, sweep, subtile).
+template <int M>
+__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep_batch(BatchSweepArgs a) {
+  extern __shared__ __align__(16) uint64_t vals[];
+  __shared__ unsigned long long acc[M];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ unsigned long long s_item, s_local;
+  __shared__ uint32_t s_circ;
+  SweepCta k;
+  sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc);
+  const uint32_t subtiles = kTileWords / M;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned long long it = atomicAdd(a.queue, 1ull);
+      s_item = it;
+      if (it < a.n_items) {  // circuit holding the item: last prefix <= it
+        const uint32_t lo = find_prefix(a.item_prefix, a.n_circ, it);
+        s_circ = a.circ_ids[lo];
+        s_local = it - a.item_prefix[lo];
+      }
     }
     __syncthreads();
-    if (tid < M) a.out[(uint64_t)si * 32 + w0 + tid] = acc[tid];
+    const unsigned long long item = s_item;
+    const uint32_t ci = s_circ;
+    const unsigned long long local = s_local;
+    __syncthreads();
+    if (item >= a.n_items) return;
+    const BatchCirc& c = a.circs[ci];
+    const uint64_t per_tile = (uint64_t)c.n_sweeps * subtiles;
+    const uint32_t tile = (uint32_t)(local / per_tile);
+    const uint64_t rem = local % per_tile;
+    const uint32_t si = (uint32_t)(rem / subtiles);
+    const uint32_t w0 = (uint32_t)(rem % subtiles) * M;
+    const SweepView v{c.recs, c.level, c.level_off, c.li_off, c.li, c.fi_off, c.fi_idx, c.type,
+                      c.good + (uint64_t)tile * c.N * 32, c.max_gate_level};
+    if (!sweep_item<M>(k, v, c.inj[si], w0, c.out + ((uint64_t)tile * c.n_sweeps + si) * 32)) {
+      if (threadIdx.x == 0) atomicExch(a.err, 1);
+      return;
+    }
   }
 }
 
 // ---------------------------------------------------------------- FFR tracing
 // Bits where flipping input `pin` of element p flips p's output, for bitwise
 // gate types (MUX never reaches this path).
-__device__ __forceinline__ uint64_t local_sens(const FfrArgs& a, uint32_t p, uint32_t pin,
-                                               uint32_t lane) {
+template <class V>
+__device__ __forceinline__ uint64_t local_sens(const V& a, uint32_t p, uint32_t pin, uint32_t lane) {
   const uint8_t t = a.type[p];
   if (t == G_XOR || t == G_XNOR) return ~0ull;
   if (t == G_INV || t == G_CLKBUF || t == G_PO) return pin == 0 ? ~0ull : 0ull;
@@ -488,6 +587,105 @@ __global__ void __launch_bounds__(256) k_exact(ExactArgs a) {
   record(a.count, a.first, a.lastflag, f, D, w, bits, a.W, lane);
 }
 
+// ---------------------------------------------------------------- batches
+// The good-machine words and scratch of one circuit's tile, for the batched
+// tracing kernels.
+struct TileView {
+  const uint8_t* type;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint64_t* good;
+};
+
+// One warp per (element, tile) of a level, over the circuits of the batch.
+__global__ void __launch_bounds__(256) k_good_batch(const BatchCirc* circs, const BatchGoodSeg* segs,
+                                                    uint32_t n_segs, unsigned long long n_units) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long unit = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (unit >= n_units) return;
+  uint32_t lo = 0, hi = n_segs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (segs[mid].unit0 <= unit) lo = mid; else hi = mid;
+  }
+  const BatchGoodSeg sg = segs[lo];
+  const BatchCirc& c = circs[sg.circ];
+  const unsigned long long local = unit - sg.unit0;
+  const uint32_t e = sg.lo + (uint32_t)(local / c.tiles);
+  const uint32_t tile = (uint32_t)(local % c.tiles);
+  const uint32_t w = tile * 32 + lane;
+  const uint64_t base = (uint64_t)tile * c.N;
+  const uint8_t t = c.type[e];
+  uint64_t v;
+  if (t == G_PI) {
+    v = (w < c.W) ? c.pwords[(uint64_t)w * c.n_pi + e] : 0ull;
+  } else {
+    const uint32_t f0 = c.fi_off[e];
+    uint32_t nf = c.fi_off[e + 1] - f0;
+    if (t == G_INV || t == G_CLKBUF || t == G_PO) nf = 1;
+    uint64_t in[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if ((uint32_t)k < nf) in[k] = c.good[(base + c.fi_idx[f0 + k]) * 32 + lane];
+    v = eval_word(t, nf, in[0], in[1], in[2], in[3]);
+  }
+  c.good[(base + e) * 32 + lane] = v;
+}
+
+// One warp per (circuit, tile, root): the k_ffr body on that circuit's tile.
+__global__ void __launch_bounds__(256) k_ffr_batch(BatchUnits u, unsigned long long n_units) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long unit = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (unit >= n_units) return;
+  const uint32_t ci = find_prefix(u.unit_prefix, u.n_circ, unit);
+  const BatchCirc& c = u.circs[ci];
+  const unsigned long long local = unit - u.unit_prefix[ci];
+  const uint32_t tile = (uint32_t)(local / c.n_roots);
+  const uint32_t ri = (uint32_t)(local % c.n_roots);
+  const TileView tv{c.type, c.fi_off, c.fi_idx, c.good + (uint64_t)tile * c.N * 32};
+  uint64_t* sens = c.sens + (uint64_t)tile * c.N * 32;
+  const uint64_t* obsv = c.out + (uint64_t)tile * c.n_sweeps * 32;
+  const RootRec rr = c.roots[ri];
+  const uint32_t w = tile * 32 + lane;
+  const uint32_t bits = round_bits(c.P, c.W, w);
+  uint64_t obs = rr.obs == kObsOne ? ~0ull : rr.obs == kObsZero ? 0ull : obsv[(uint64_t)rr.obs * 32 + lane];
+  obs &= bits_mask(bits);
+  sens[(uint64_t)rr.root * 32 + lane] = ~0ull;
+  for (uint32_t i = rr.mem_begin; i < rr.mem_end; ++i) {
+    const MemberRec m = c.members[i];
+    sens[(uint64_t)m.e * 32 + lane] = sens[(uint64_t)m.p * 32 + lane] & local_sens(tv, m.p, m.pin, lane);
+  }
+  for (uint32_t i = rr.flt_begin; i < rr.flt_end; ++i) {
+    const TracedRec tr = c.traced[i];
+    uint64_t sv, gv;
+    if (tr.pin == 0) {
+      sv = sens[(uint64_t)tr.elem * 32 + lane];
+      gv = tv.good[(uint64_t)tr.elem * 32 + lane];
+    } else {
+      sv = sens[(uint64_t)tr.elem * 32 + lane] & local_sens(tv, tr.elem, tr.pin - 1, lane);
+      gv = tv.good[(uint64_t)c.fi_idx[c.fi_off[tr.elem] + tr.pin - 1] * 32 + lane];
+    }
+    const uint64_t D = sv & (gv ^ (tr.value ? ~0ull : 0ull)) & obs;
+    record(c.count, c.first, c.lastflag, tr.fault, D, w, bits, c.W, lane);
+  }
+}
+
+// One warp per (circuit, tile, exact fault).
+__global__ void __launch_bounds__(256) k_exact_batch(BatchUnits u, unsigned long long n_units) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long unit = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (unit >= n_units) return;
+  const uint32_t ci = find_prefix(u.unit_prefix, u.n_circ, unit);
+  const BatchCirc& c = u.circs[ci];
+  const unsigned long long local = unit - u.unit_prefix[ci];
+  const uint32_t tile = (uint32_t)(local / c.n_exact);
+  const uint32_t j = (uint32_t)(local % c.n_exact);
+  const uint32_t w = tile * 32 + lane;
+  const uint32_t bits = round_bits(c.P, c.W, w);
+  const uint64_t D = c.out[((uint64_t)tile * c.n_sweeps + c.n_stem_sweeps + j) * 32 + lane] & bits_mask(bits);
+  record(c.count, c.first, c.lastflag, c.exact_fault[j], D, w, bits, c.W, lane);
+}
+
 __global__ void k_init_results(unsigned long long* count, unsigned long long* first,
                                uint8_t* lastflag, uint32_t F) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
@@ -539,6 +737,59 @@ __global__ void k_drop(DropArgs a) {
 }
 
 }  // namespace
+
+void launch_good_batch(const BatchCirc* circs, const BatchGoodSeg* segs, uint32_t n_segs,
+                       unsigned long long n_units, cudaStream_t s) {
+  if (!n_units) return;
+  k_good_batch<<<(unsigned)((n_units * 32 + 255) / 256), 256, 0, s>>>(circs, segs, n_segs, n_units);
+}
+
+void launch_ffr_batch(const BatchUnits& u, unsigned long long n_units, cudaStream_t s) {
+  if (!n_units) return;
+  k_ffr_batch<<<(unsigned)((n_units * 32 + 255) / 256), 256, 0, s>>>(u, n_units);
+}
+
+void launch_exact_batch(const BatchUnits& u, unsigned long long n_units, cudaStream_t s) {
+  if (!n_units) return;
+  k_exact_batch<<<(unsigned)((n_units * 32 + 255) / 256), 256, 0, s>>>(u, n_units);
+}
+
+void launch_init_results_batch(unsigned long long* count, unsigned long long* first, uint8_t* lastflag,
+                               uint64_t F, cudaStream_t s) {
+  if (!F) return;
+  const uint64_t blocks = std::min<uint64_t>((F + 255) / 256, 4096);
+  k_init_results<<<(unsigned)blocks, 256, 0, s>>>(count, first, lastflag, (uint32_t)std::min<uint64_t>(F, 0xFFFFFFFFull));
+}
+
+#define FSIMB_SWEEP_BATCH_CASES(X) X(1) X(2) X(4) X(8)
+cudaError_t sweep_batch_set_smem(int M, size_t smem) {
+  switch (M) {
+#define X(m) case m: return cudaFuncSetAttribute(k_sweep_batch<m>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    FSIMB_SWEEP_BATCH_CASES(X)
+#undef X
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t sweep_batch_occupancy(int M, int threads, size_t smem, int* blocks_per_sm) {
+  switch (M) {
+#define X(m) case m: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_sweep_batch<m>, threads, smem);
+    FSIMB_SWEEP_BATCH_CASES(X)
+#undef X
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepArgs& a,
+                               cudaStream_t s) {
+  switch (M) {
+#define X(m) case m: k_sweep_batch<m><<<blocks, threads, smem, s>>>(a); break;
+    FSIMB_SWEEP_BATCH_CASES(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
 
 void launch_good_level(const GoodArgs& a, cudaStream_t s) {
   const uint64_t n = (uint64_t)(a.hi - a.lo) * a.W_pad;

@@ -95,6 +95,74 @@ struct DropArgs {
   uint32_t* n_out;           // [3]: roots, sweeps, exact
 };
 
+// ---------------------------------------------------------------- batches
+// One circuit of a batch: device pointers into the batch's concatenated
+// arrays and the circuit's sizes.
+struct BatchCirc {
+  const uint4* recs;
+  const uint32_t* level;
+  const uint32_t* level_off;
+  const uint32_t* li_off;
+  const uint32_t* li;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const InjRec* inj;
+  const RootRec* roots;
+  const MemberRec* members;
+  const TracedRec* traced;
+  const uint32_t* exact_fault;
+  const uint64_t* pwords;        // [W][n_pi]
+  uint64_t* good;                // [tiles][N][32]
+  uint64_t* out;                 // [tiles][n_sweeps][32]
+  uint64_t* sens;                // [tiles][N][32]
+  unsigned long long* count;     // per fault
+  unsigned long long* first;
+  uint8_t* lastflag;
+  uint64_t P;
+  uint32_t N, n_pi, W, tiles;
+  uint32_t n_sweeps, n_stem_sweeps, n_roots, n_exact;
+  uint32_t max_gate_level, n_levels;
+};
+
+struct BatchSweepArgs {
+  const BatchCirc* circs;
+  const uint32_t* circ_ids;                  // circuits of this launch, in item order
+  const unsigned long long* item_prefix;     // [n_circ] first item of each; items of a
+                                             // circuit are (tile, sweep, subtile), tile-major
+  uint32_t n_circ;
+  unsigned long long n_items;
+  unsigned long long* queue;
+  uint32_t vals_bytes, rec_buf;
+  int* err;
+};
+
+// A level of the batched good machine: segments (circuit, element range)
+// with one warp per (element, tile).
+struct BatchGoodSeg {
+  uint32_t circ, lo, hi, pad;
+  unsigned long long unit0;  // first unit of the segment
+};
+
+// Units of the batched tracing kernels: one warp per (circuit, tile, root)
+// or (circuit, tile, exact fault); prefix over circuits.
+struct BatchUnits {
+  const BatchCirc* circs;
+  const unsigned long long* unit_prefix;  // [n_circ + 1]
+  uint32_t n_circ;
+};
+
+void launch_good_batch(const BatchCirc* circs, const BatchGoodSeg* segs, uint32_t n_segs,
+                       unsigned long long n_units, cudaStream_t s);
+cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepArgs& a,
+                               cudaStream_t s);
+cudaError_t sweep_batch_set_smem(int M, size_t smem);
+cudaError_t sweep_batch_occupancy(int M, int threads, size_t smem, int* blocks_per_sm);
+void launch_ffr_batch(const BatchUnits& u, unsigned long long n_units, cudaStream_t s);
+void launch_exact_batch(const BatchUnits& u, unsigned long long n_units, cudaStream_t s);
+void launch_init_results_batch(unsigned long long* count, unsigned long long* first, uint8_t* lastflag,
+                               uint64_t F, cudaStream_t s);
+
 void launch_good_level(const GoodArgs& a, cudaStream_t s);
 // Returns cudaErrorInvalidValue when M is unsupported.
 cudaError_t launch_sweep(int M, int threads, int blocks, size_t smem, const SweepArgs& a,

@@ -210,6 +210,17 @@ class Simulator:
             v.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n))
         return s, p, v
 
+    def dot(self):
+        """Graphviz text of the circuit (the reference's visualization_graph layout)."""
+        ptr, n = ctypes.c_void_p(), ctypes.c_size_t()
+        self._check(_lib.lib().fsimb_dot(self._h, ctypes.byref(ptr), ctypes.byref(n)))
+        return _lib.take_text(ptr, n)
+
+    def visualization_graph(self, output_file):
+        """Writes dot() to a file, like fsim::Simulator::visualization_graph."""
+        with open(output_file, "w") as f:
+            f.write(self.dot())
+
     def patterns(self):
         i = self.info()
         out = np.zeros(i.num_rounds * i.num_pis, dtype=np.uint64)

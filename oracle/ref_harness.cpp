@@ -194,6 +194,11 @@ void ref_arrays(void* hp, uint64_t* tpg, uint64_t* levels, uint64_t* per_level,
   }
 }
 
+// Public entry point: Simulator::visualization_graph(path).
+void ref_visualize(void* hp, const char* path) {
+  ((ref_handle*)hp)->sim.visualization_graph(path);
+}
+
 // Public entry point: Simulator::run(mode, threads).
 void ref_run_table(void* hp, int mode, int threads, uint64_t* table, uint64_t* good) {
   auto& s = ((ref_handle*)hp)->sim;

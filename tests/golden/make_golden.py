@@ -5,7 +5,9 @@
    (unittests/test_basics.cpp:8-345).  The C string literals there use
    backslash-newline continuations, which the compiler removes; the strings
    are stored as the compiler sees them.
-2. ``ref_cases.json``: small synthetic circuits (all gate types including
+2. ``test_basics_dot.json``: the reference's Graphviz output
+   (Simulator::visualization_graph) for those seven fixtures.
+3. ``ref_cases.json``: small synthetic circuits (all gate types including
    XNOR, CLKBUF and MUX, several rounds, partial last rounds) run through the
    reference's own simulator compiled into ``oracle/_ref`` (``make -C oracle
    ref``), recording per-fault detected / first / count, the reference's
@@ -123,8 +125,30 @@ def ref_cases():
             "cases": out}
 
 
+def ref_dot(tb):
+    """The reference's visualization_graph output for each unit-test fixture."""
+    import tempfile
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libfsim_ref.so"))
+    lib.ref_load_text.restype = ctypes.c_void_p
+    lib.ref_load_text.argtypes = [ctypes.c_char_p, ctypes.c_size_t] * 3
+    lib.ref_visualize.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    lib.ref_free.argtypes = [ctypes.c_void_p]
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        for c in tb["cases"]:
+            ck, fl, pt = c["ckt"].encode(), c["flst"].encode(), c["ptn"].encode()
+            h = lib.ref_load_text(ck, len(ck), fl, len(fl), pt, len(pt))
+            path = os.path.join(d, "g.dot")
+            lib.ref_visualize(h, path.encode())
+            out.append({"name": c["name"], "dot": open(path).read()})
+            lib.ref_free(h)
+    return {"source": "fsim::Simulator::visualization_graph via oracle/_ref", "cases": out}
+
+
 def main():
     tb = extract_test_basics()
+    with open(os.path.join(HERE, "test_basics_dot.json"), "w") as f:
+        json.dump(ref_dot(tb), f, indent=1)
     with open(os.path.join(HERE, "test_basics_golden.json"), "w") as f:
         json.dump(tb, f, indent=1)
     rc = ref_cases()

@@ -156,3 +156,13 @@ def test_collapsed_faults_are_equivalent_classes():
     sig_col = {(int(a), int(b)) for a, b in zip(rc["count"], rc["first"])}
     assert sig_full == sig_col
     assert len(col.faults) < len(full.faults)
+
+
+def test_dot_matches_reference_visualization(basics):
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "test_basics_dot.json")) as f:
+        dots = json.load(f)["cases"]
+    for c, d in zip(basics["cases"], dots):
+        sim = Simulator(-1)
+        sim.read_text(c["ckt"], c["flst"], c["ptn"])
+        assert sim.dot() == d["dot"], c["name"]
