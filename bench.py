@@ -17,6 +17,13 @@ With N > 1 each rank simulates its own 65,536-pattern block (seed = rank)
 and the per-fault results are merged across ranks every step (weak scaling).
 --impl reference times LSIM's own CPU simulator (oracle/_ref, else the CPU
 port in oracle/) on a bounded sample of the same workload on all host cores.
+
+--workload c4 times the batched configuration instead: 256 circuits
+(gen.batch_configs: 500-50,000 gates log-uniform, 10-120 levels, SA0/SA1 on
+every gate output, 1,024-16,384 patterns) run as one batch (fsimb_batch_*,
+CUDA graph, autotuned sweep shape) against the same 256 circuits run one
+after another through the plain per-circuit path, both with inputs resident
+(value) and with every input copied from host memory each step (e2e).
 """
 import argparse
 import json
@@ -229,8 +236,10 @@ def run_ours(args):
         return shard.merge_results(res, rank * P, rank == world - 1, world * info.num_rounds,
                                    device="cuda")
 
+    tune_ms = 0.0
     for _ in range(args.warmup):
-        sim.run(stream=sp)
+        sim.run(stream=sp, tune=True)  # the first run tunes the sweep shape
+        tune_ms += sim.stats()["ms_tune"]
         merge(sim.results())
     torch.cuda.synchronize()
 
@@ -244,7 +253,7 @@ def run_ours(args):
     e0.record(stream)
     sweep_ms, sweep_bytes, tiles, launches = 0.0, 0, 0, 0
     for _ in range(args.steps):
-        sim.run(stream=sp)
+        sim.run(stream=sp, tune=True)
         merged = merge(sim.results())
         st = sim.stats()
         sweep_ms += st["ms_sweep"]
@@ -270,7 +279,7 @@ def run_ours(args):
     g0.record(stream)
     for _ in range(args.steps):
         sim.set_patterns(host_words, P)
-        sim.run(stream=sp)
+        sim.run(stream=sp, tune=True)
         merged = merge(sim.results())
     g1.record(stream)
     torch.cuda.synchronize()
@@ -300,7 +309,10 @@ def run_ours(args):
                          % (info.num_elements * info.num_rounds * 8 / 1e9),
                    "sweep": {"words_per_item": st["words_per_item"],
                              "block_threads": st["block_threads"], "blocks": st["blocks"],
-                             "smem_bytes": st["smem_bytes"], "max_live": st["max_live"]}},
+                             "ctas_per_sm": st["ctas_per_sm"], "smem_bytes": st["smem_bytes"],
+                             "max_live": st["max_live"],
+                             "shape": "autotuned during warm-up on a strided sample of the "
+                                      "first tile's sweeps", "tune_ms": tune_ms}},
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": int(words.nbytes),
                 "d2h_bytes_per_step": int(F * 17)},
@@ -324,6 +336,124 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """Batched configuration: one batch of 256 circuits against 256 plain runs."""
+    import torch
+    from lsim_b200 import Batch, Simulator, gen
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    cfgs = gen.batch_configs(args.circuits, seed=0)
+    t0 = time.perf_counter()
+    ws = [gen.generate(**c) for c in cfgs]
+    gen_s = time.perf_counter() - t0
+    members, plains = [], []
+    for w in ws:
+        m = Simulator(-1)
+        m.read_text(w["ckt"], w["flst"], w["ptn"])
+        members.append(m)
+        p = Simulator(0)
+        p.read_text(w["ckt"], w["flst"], w["ptn"])
+        plains.append(p)
+    F = sum(m.info().num_faults for m in members)
+    FP = sum(m.info().num_faults * m.info().num_patterns for m in members)
+    gates = [c["n_gates"] for c in cfgs]
+    b = Batch(0)
+    for m in members:
+        b.add(m)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # warm-up: the first batch run tunes the sweep shape and captures the graph
+    t0 = time.perf_counter()
+    b.run(tune=True, stream=sp)
+    first_s = time.perf_counter() - t0
+    tune_ms = b.stats()["ms_tune"]
+    for _ in range(max(0, args.warmup - 1)):
+        b.run(tune=True, stream=sp)
+    for p in plains:
+        p.run(stream=sp, tune=True)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_batch = timed(lambda: b.run(tune=True, stream=sp), args.steps)
+    st = b.stats()
+    ms_serial = timed(lambda: b.run(tune=True, concurrent=False, stream=sp), args.steps)
+    ms_plain = timed(lambda: [p.run(stream=sp, tune=True) for p in plains], args.steps)
+    clk = clocks.stop()
+    plain_launches = sum(p.stats()["kernel_launches"] for p in plains)
+    # e2e: every input from host memory each step
+    ms_batch_e2e = timed(lambda: b.run(tune=True, reupload=True, stream=sp), args.steps)
+    st_e2e = b.stats()
+    words = [p.patterns() for p in plains]
+    pinned = [torch.from_numpy(wd.ravel()).pin_memory().numpy() for wd in words]
+
+    def plain_e2e():
+        for p, wd, m in zip(plains, pinned, members):
+            p.set_patterns(wd, m.info().num_patterns)
+            p.run(stream=sp, tune=True)
+            p.results()
+    ms_plain_e2e = timed(plain_e2e, args.steps)
+    # phase split of one step of each arm (batch without the graph)
+    b.run(tune=True, graph=False, stream=sp)
+    st_ng = b.stats()
+    classes = b.classes()
+    phases = {"batch": {k: st_ng[k] for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")},
+              "plain": {k: sum(p.stats()[k] for p in plains)
+                        for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")}}
+    # results agree with the plain path on every circuit
+    same = all(np.array_equal(m.results(), p.results()) for m, p in zip(members, plains))
+    peak, peak_src = _peaks()
+    sweep_s = st["ms_compute"] / 1e3
+    line = {
+        "metric": "fault×pattern evals/s (batched, %d circuits)" % args.circuits,
+        "value": FP * args.steps / (ms_batch / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic",
+        "config": {"workload": "c4: %d circuits, %d-%d gates (median %d), 10-120 levels, SA0/SA1 "
+                               "on every gate output (%d faults), 1,024-16,384 patterns"
+                               % (args.circuits, min(gates), max(gates), int(np.median(gates)), F),
+                   "fault_patterns_per_step": FP, "mode": "count",
+                   "sweep": {k: st[k] for k in ("words_per_item", "block_threads", "ctas_per_sm",
+                                                "blocks", "smem_bytes", "n_classes")},
+                   "graph": bool(st["graph_used"]), "tune_ms": tune_ms,
+                   "first_run_s": first_s, "generate_s": gen_s},
+        "plain_sequential": {"value": FP * args.steps / (ms_plain / 1e3),
+                             "ms_per_step": ms_plain / args.steps,
+                             "gpu_launches_per_step": int(plain_launches)},
+        "batch_over_plain": ms_plain / ms_batch,
+        "batch_serial_classes": {"value": FP * args.steps / (ms_serial / 1e3),
+                                 "ms_per_step": ms_serial / args.steps},
+        "e2e": {"value": FP * args.steps / (ms_batch_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": int(st_e2e["h2d_bytes"]),
+                "d2h_bytes_per_step": int(st_e2e["d2h_bytes"])},
+        "plain_sequential_e2e": {"value": FP * args.steps / (ms_plain_e2e / 1e3),
+                                 "ms_per_step": ms_plain_e2e / args.steps},
+        "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "breakdown_ms_per_step": {"compute": st["ms_compute"], "d2h": st["ms_d2h"],
+                                  "total": st["ms_total"]},
+        "roofline": {"bound": "hbm", "achieved": st["sweep_alg_bytes"] / sweep_s / 1e9,
+                     "peak": peak, "unit": "GB/s",
+                     "frac": st["sweep_alg_bytes"] / sweep_s / 1e9 / peak, "traffic": None,
+                     "kernel": "whole batch (good + sweeps + tracing)",
+                     "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "phases_ms_per_step": phases,
+        "classes": classes,
+        "results_equal_plain": same,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,6 +463,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
+    ap.add_argument("--circuits", type=int, default=256, help="batch size for --workload c4")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed run of the workload (for profiler captures)")
     args = ap.parse_args()
@@ -349,6 +480,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c4":
+        run_batch(args)
     else:
         run_ours(args)
 

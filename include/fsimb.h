@@ -54,6 +54,11 @@ typedef struct {
                                 it (first_pattern exact, count covers that tile) */
   uint32_t words_per_item;   /* sweep words per work item: 0 auto, or 1,2,4,8 */
   uint32_t block_threads;    /* sweep CTA size: 0 auto, or a multiple of 32 up to 1024 */
+  uint32_t ctas_per_sm;      /* sweep CTAs sharing an SM: 0 auto, or 1..8; sizes the
+                                record buffer so that many fit */
+  uint32_t tune;             /* 1, with the three above 0: on the first run of a circuit and
+                                fault list, time candidate sweep shapes on a strided sample
+                                of the first tile's sweeps and keep the fastest */
   void* stream;              /* cudaStream_t to run on; NULL: the handle's stream */
 } fsimb_opts;
 
@@ -86,6 +91,9 @@ typedef struct {
   double ms_compute;         /* device time from results init to the last tile */
   uint64_t bank_conflict_groups; /* sweep access groups whose slots share a bank position */
   uint64_t bank_access_groups;   /* sweep access groups (fanin loads and stores) per item */
+  double ms_tune;            /* shape autotuning inside this run (0 when reused) */
+  uint32_t ctas_per_sm;      /* sweep CTAs resident per SM */
+  uint32_t pad;
 } fsimb_stats;
 
 /* Lifecycle.  fsimb_create fails with FSIMB_ERR_CUDA when `device` is not a
@@ -174,6 +182,76 @@ int fsimb_dot(const fsimb_handle* h, char** text, size_t* len);
  * after the kernels are enqueued on `stream` (NULL: the handle's stream). */
 int fsimb_good_po_noalloc(fsimb_handle* h, const uint64_t* d_pattern_words, uint32_t n_words,
                           uint64_t* d_po_words, void* stream);
+
+/* ------------------------------------------------------------------ batches
+ * Many circuits, each with its own fault list and pattern block, simulated
+ * together.  No counterpart in the reference, whose drivers simulate one
+ * circuit per process (main/simple.cpp:21-39, main/MA_partition.cu:40-63).
+ * One run launches, for all members at once: the good machine one launch per
+ * level index, the sweeps as one persistent launch per words-per-item class
+ * pulling (circuit, tile, sweep, subtile) items from a device work counter,
+ * and one launch each for FFR tracing and exact faults.  The sequence is
+ * captured into a CUDA graph and replayed while the membership stays the same.
+ * Members are handles loaded with circuit, faults and patterns; host-only
+ * handles (device -1) are enough.  The batch borrows them until
+ * fsimb_batch_clear or fsimb_batch_destroy and writes each member's results
+ * into it (read them with fsimb_results / fsimb_found_fault_to_pattern);
+ * they equal what fsimb_run gives in count mode.  Changing a member's inputs
+ * between runs is allowed: the batch notices and lays out again. */
+typedef struct fsimb_batch fsimb_batch;
+
+typedef struct {
+  uint32_t struct_size;
+  uint32_t words_per_item;   /* 0 auto, or 1, 2, 4, 8 (members whose live values
+                                do not fit take the next smaller value) */
+  uint32_t block_threads;    /* 0 auto, or a multiple of 32 up to 1024 */
+  uint32_t ctas_per_sm;      /* 0 auto (1), or 1..4: sizes the sweep CTA's record buffer */
+  uint32_t tune;             /* 1, with the three above 0: time candidate shapes on a
+                                sample of the batch (the first tile of a spread of its
+                                circuits) the first time a membership runs; the winner
+                                is kept until the membership changes */
+  uint32_t no_graph;         /* 1: launch the kernels directly instead of through a graph */
+  uint32_t reupload;         /* 1: copy every member's inputs (circuit, plan, patterns)
+                                from host memory again even if none changed */
+  uint32_t serial_classes;   /* 1: run the sweep classes one after another instead of
+                                as concurrent branches */
+  void* stream;              /* cudaStream_t; NULL: the batch's stream */
+} fsimb_batch_opts;
+
+typedef struct {
+  double ms_total;           /* layout upload + kernels + result copies */
+  double ms_h2d, ms_compute, ms_d2h;
+  double ms_good, ms_sweep, ms_ffr;  /* phases, when run without the graph */
+  double ms_tune;            /* autotuner time in this run (0 when reused) */
+  double ms_host_prep;       /* host planning and scheduling in this run */
+  uint64_t n_circuits, n_faults;
+  uint64_t fault_patterns;   /* sum over members of faults x patterns */
+  uint64_t sweep_items, ffr_units, exact_units, good_units;
+  uint64_t dense_gate_words, sweep_alg_bytes, good_gate_words;
+  uint64_t kernel_launches;  /* kernels in the launch sequence */
+  uint32_t graph_used, n_classes;
+  uint32_t words_per_item, block_threads, blocks, smem_bytes, ctas_per_sm;  /* largest class */
+  uint32_t pad;
+  uint64_t device_bytes;
+  uint64_t h2d_bytes, d2h_bytes;  /* host<->device bytes copied by this run */
+} fsimb_batch_stats;
+
+int fsimb_batch_create(int device, fsimb_batch** out);
+int fsimb_batch_destroy(fsimb_batch* b);
+const char* fsimb_batch_last_error(const fsimb_batch* b);
+int fsimb_batch_add(fsimb_batch* b, fsimb_handle* member);
+int fsimb_batch_clear(fsimb_batch* b);
+int fsimb_batch_size(const fsimb_batch* b, uint64_t* n);
+int fsimb_batch_run(fsimb_batch* b, const fsimb_batch_opts* opts);
+int fsimb_batch_get_stats(const fsimb_batch* b, fsimb_batch_stats* out);
+/* Sweep classes of the last run: circuits sharing one sweep launch shape. */
+typedef struct {
+  uint32_t words_per_item, block_threads, blocks, smem_bytes;
+  uint64_t n_circuits, sweep_items;
+  uint32_t max_live, widest_level;
+  double ms_sweep;           /* the class's launch, when run without the graph */
+} fsimb_batch_class;
+int fsimb_batch_class_stats(const fsimb_batch* b, uint32_t index, fsimb_batch_class* out);
 
 /* Synthetic workloads (seeded; text in LSIM's formats).  Returned buffers
  * are released with fsimb_free_text. */

@@ -33,6 +33,7 @@ class FaultResult(ctypes.Structure):
 class Opts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("drop", ctypes.c_uint32),
                 ("words_per_item", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("ctas_per_sm", ctypes.c_uint32), ("tune", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p)]
 
 
@@ -53,7 +54,8 @@ class Stats(ctypes.Structure):
                  ["words_per_item", "block_threads", "blocks", "smem_bytes"]] +
                 [("device_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
                  ("ms_compute", ctypes.c_double), ("bank_conflict_groups", ctypes.c_uint64),
-                 ("bank_access_groups", ctypes.c_uint64)])
+                 ("bank_access_groups", ctypes.c_uint64), ("ms_tune", ctypes.c_double),
+                 ("ctas_per_sm", ctypes.c_uint32), ("pad", ctypes.c_uint32)])
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -68,6 +70,43 @@ class GenConfig(ctypes.Structure):
                 ("hub_fo_min", ctypes.c_uint32), ("hub_fo_max", ctypes.c_uint32),
                 ("fo_min", ctypes.c_uint32), ("fo_max", ctypes.c_uint32),
                 ("p_unused", ctypes.c_double), ("shuffle_ids", ctypes.c_int32)]
+
+
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("words_per_item", ctypes.c_uint32),
+                ("block_threads", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
+                ("tune", ctypes.c_uint32), ("no_graph", ctypes.c_uint32),
+                ("reupload", ctypes.c_uint32), ("serial_classes", ctypes.c_uint32),
+                ("stream", ctypes.c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in
+                 ["ms_total", "ms_h2d", "ms_compute", "ms_d2h", "ms_good", "ms_sweep", "ms_ffr",
+                  "ms_tune", "ms_host_prep"]] +
+                [(n, ctypes.c_uint64) for n in
+                 ["n_circuits", "n_faults", "fault_patterns", "sweep_items", "ffr_units",
+                  "exact_units", "good_units", "dense_gate_words", "sweep_alg_bytes",
+                  "good_gate_words", "kernel_launches"]] +
+                [(n, ctypes.c_uint32) for n in
+                 ["graph_used", "n_classes", "words_per_item", "block_threads", "blocks",
+                  "smem_bytes", "ctas_per_sm", "pad"]] +
+                [("device_bytes", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64),
+                 ("d2h_bytes", ctypes.c_uint64)])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad"}
+
+
+class BatchClass(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_uint32) for n in
+                 ["words_per_item", "block_threads", "blocks", "smem_bytes"]] +
+                [("n_circuits", ctypes.c_uint64), ("sweep_items", ctypes.c_uint64),
+                 ("max_live", ctypes.c_uint32), ("widest_level", ctypes.c_uint32),
+                 ("ms_sweep", ctypes.c_double)])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 # Every symbol the header declares, with its ctypes signature.
@@ -110,6 +149,15 @@ SIGNATURES = {
     "fsimb_dot": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ)]),
     "fsimb_good_po_noalloc": (ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                              ctypes.c_void_p]),
+    "fsimb_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "fsimb_batch_destroy": (ctypes.c_int, [_P]),
+    "fsimb_batch_last_error": (_CP, [_P]),
+    "fsimb_batch_add": (ctypes.c_int, [_P, _P]),
+    "fsimb_batch_clear": (ctypes.c_int, [_P]),
+    "fsimb_batch_size": (ctypes.c_int, [_P, _U64P]),
+    "fsimb_batch_run": (ctypes.c_int, [_P, ctypes.POINTER(BatchOpts)]),
+    "fsimb_batch_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
+    "fsimb_batch_class_stats": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(BatchClass)]),
 }
 
 _lib = None
@@ -131,9 +179,9 @@ def lib():
     return _lib
 
 
-def check(code, handle=None):
+def check(code, handle=None, last_error="fsimb_last_error"):
     if code != OK:
-        msg = lib().fsimb_last_error(handle)
+        msg = getattr(lib(), last_error)(handle)
         raise FsimbError(code, msg.decode() if msg else "")
 
 

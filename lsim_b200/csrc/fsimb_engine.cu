@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -51,6 +52,185 @@ std::string read_file(const char* path) {
 }  // namespace
 
 // --------------------------------------------------------------------------
+static int m_slot(int M) { return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : 3; }
+
+const Schedule& fsimb_handle::cached_schedule(int M) {
+  const int sl = m_slot(M);
+  if (sched_cache_gen[sl] != plan_gen) {
+    if (sched_M == M) {
+      sched_cache[sl] = sched;
+    } else {
+      build_schedule(nl, plan, 16u / (uint32_t)M, sched_cache[sl]);
+    }
+    sched_cache_gen[sl] = plan_gen;
+  }
+  return sched_cache[sl];
+}
+
+void fsimb_handle::use_schedule(int M) {
+  if (sched_M == M) return;
+  sched = cached_schedule(M);
+  sched_M = M;
+  sched_uploaded = false;
+}
+
+void fsimb_handle::default_shape(std::vector<uint32_t> widths, uint32_t widest, int& M, int& occ,
+                                 int& threads) {
+  M = 0;
+  occ = 1;
+  threads = 0;
+  const size_t share2 = sweep_smem_share(smem_optin, smem_per_sm, 2);
+  for (int m : {8, 4}) {
+    // plan.max_live (no bank constraints) bounds every schedule's slots from below
+    if (sweep_vals_bytes(plan.max_live, m) + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
+    const Schedule& sc = cached_schedule(m);
+    if (sc.max_live > kMaxSlots) continue;
+    const uint32_t vals = sweep_vals_bytes(sc.max_live, m);
+    if (vals + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
+    const size_t smem = vals + std::min<size_t>(widest, (share2 - vals) / 32) * 32;
+    CK(sweep_set_smem(m, smem));
+    int t = (int)std::min<uint32_t>(pick_sweep_threads(widths, m), sweep_max_threads(m));
+    for (; t > 64; t -= 32) {
+      int got = 0;
+      CK(sweep_occupancy(m, t, smem, &got));
+      if (got >= 2) break;
+    }
+    M = m;
+    occ = 2;
+    threads = t;
+    return;
+  }
+}
+
+void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& widths, uint32_t widest) {
+  const uint32_t N = plan.N;
+  const uint32_t n_sweeps = (uint32_t)plan.sweeps.size();
+  for (auto& e : tune_ev)
+    if (!e) CK(cudaEventCreate(&e));
+  // good machine of tile 0
+  for (uint32_t l = 0; l < nl.n_levels; ++l) {
+    GoodArgs g{};
+    g.type = d_type.as<uint8_t>();
+    g.fi_off = d_fi_off.as<uint32_t>();
+    g.fi_idx = d_fi_idx.as<uint32_t>();
+    g.pwords = d_pwords.as<uint64_t>();
+    g.good = d_good.as<uint64_t>();
+    g.n_pi = (uint32_t)nl.n_pi;
+    g.N = N;
+    g.lo = nl.level_off[l];
+    g.hi = nl.level_off[l + 1];
+    g.W = (uint32_t)pats.W;
+    g.W_pad = kTileWords;
+    launch_good_level(g, s);
+  }
+  CK(cudaGetLastError());
+  // every stride-th sweep: about 6% of them, at least 2,048 when there are
+  const uint32_t stride = std::max<uint32_t>(1, std::min<uint32_t>(16, n_sweeps / 2048));
+  std::vector<uint32_t> list;
+  for (uint32_t i = 0; i < n_sweeps; i += stride) list.push_back(i);
+  upload(d_tune_list, list, s);
+  float best_ms = 1e30f;
+  int bM = 0, bT = 0, bocc = 1;
+  // The default shape is the incumbent: a candidate replaces it only when
+  // faster by more than 2% on the sample (the sample favours no shape, but
+  // its time carries a few percent of noise).
+  int dM = 0, docc = 1, dT = 0;
+  default_shape(widths, widest, dM, docc, dT);
+  if (!dM) {
+    const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
+    dM = 8;
+    while (dM > 1 && sweep_vals_bytes(plan.max_live, dM) > share1) dM /= 2;
+    while (dM > 1 && sweep_vals_bytes(cached_schedule(dM).max_live, dM) > share1) dM /= 2;
+    std::vector<uint32_t> w(widths);
+    dT = (int)std::min<uint32_t>(pick_sweep_threads(w, dM), sweep_max_threads(dM));
+  }
+  float default_ms = -1;
+  struct Cand {
+    int M, occ, T;
+  };
+  std::vector<Cand> cands{{dM, docc, dT}};
+  for (int M : {8, 4, 2})
+    for (int occ : {1, 2, 3, 4})
+      for (int T : {128, 256, 384, 512, 768, 1024})
+        if (!(M == dM && occ == docc && T == dT)) cands.push_back({M, occ, T});
+  int cur_M = 0;
+  for (const Cand& cd : cands) {
+    const int M = cd.M, occ = cd.occ, T = cd.T;
+    const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
+    if (sweep_vals_bytes(plan.max_live, M) > share1) continue;
+    const Schedule& sc = cached_schedule(M);
+    if (sc.max_live > kMaxSlots || sweep_vals_bytes(sc.max_live, M) > share1) continue;
+    if (cur_M != M) {
+      upload(d_recs, sc.recs, s);
+      upload(d_li_off, sc.li_off, s);
+      upload(d_li, sc.li, s);
+      sched_uploaded = false;
+      cur_M = M;
+    }
+    const uint32_t vals = sweep_vals_bytes(sc.max_live, M);
+    const size_t share = sweep_smem_share(smem_optin, smem_per_sm, occ);
+    if (vals > share) continue;
+    const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (share - vals) / 32);
+    if (occ > 1 && rec_buf < std::min<uint32_t>(widest, 64)) continue;
+    const size_t smem = std::max<size_t>(16, vals + (size_t)rec_buf * 32);
+    if (T > (int)sweep_max_threads(M) || T * occ > 2048) continue;
+    CK(sweep_set_smem(M, smem));
+    int got = 0;
+    CK(sweep_occupancy(M, T, smem, &got));
+    if (got < occ) continue;  // the same as a shape with fewer CTAs per SM
+    SweepArgs sa{};
+    sa.recs = d_recs.as<uint4>();
+    sa.level = d_level.as<uint32_t>();
+    sa.level_off = d_level_off.as<uint32_t>();
+    sa.li_off = d_li_off.as<uint32_t>();
+    sa.li = d_li.as<uint32_t>();
+    sa.fi_off = d_fi_off.as<uint32_t>();
+    sa.fi_idx = d_fi_idx.as<uint32_t>();
+    sa.type = d_type.as<uint8_t>();
+    sa.inj = d_inj.as<InjRec>();
+    sa.list = d_tune_list.as<uint32_t>();
+    sa.n_list = (uint32_t)list.size();
+    sa.subtiles = kTileWords / M;
+    sa.max_gate_level = plan.max_gate_level;
+    sa.N = N;
+    sa.good = d_good.as<uint64_t>();
+    sa.out = d_out.as<uint64_t>();
+    sa.queue = d_queue.as<int>();
+    sa.vals_bytes = vals;
+    sa.rec_buf = rec_buf;
+    sa.err = d_err.as<int>();
+    const int nb = (int)std::min<uint64_t>((uint64_t)n_sms * got, (uint64_t)sa.n_list * sa.subtiles);
+    CK(cudaMemsetAsync(d_queue.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
+    CK(cudaEventRecord(tune_ev[0], s));
+    CK(launch_sweep(M, T, nb, smem, sa, s));
+    CK(cudaEventRecord(tune_ev[1], s));
+    CK(cudaEventSynchronize(tune_ev[1]));
+    int kerr = 0;
+    CK(cudaMemcpy(&kerr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+    if (default_ms < 0 && M == dM && occ == docc && T == dT) {
+      default_ms = ms;
+      best_ms = ms;
+      bM = M;
+      bT = T;
+      bocc = occ;
+    } else if (ms < (default_ms > 0 && bM == dM && bT == dT && bocc == docc ? 0.98f : 1.0f) * best_ms) {
+      best_ms = ms;
+      bM = M;
+      bT = T;
+      bocc = occ;
+    }
+  }
+  if (!bM) throw LimitError{"no sweep shape fits this circuit"};
+  tuned_M = bM;
+  tuned_T = bT;
+  tuned_occ = bocc;
+  tuned_gen = plan_gen;
+}
+
 void fsimb_handle::run(const fsimb_opts* opts) {
   if (device < 0) throw CudaError{"host-only handle: no GPU to run on"};
   if (!has_ckt || !has_faults || !has_pats) throw StateError{"load circuit, faults and patterns first"};
@@ -65,6 +245,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     throw ArgError{"words_per_item must be 0, 1, 2, 4 or 8"};
   if (o.block_threads && (o.block_threads < 32 || o.block_threads > 1024 || o.block_threads % 32))
     throw ArgError{"block_threads must be 0 or a multiple of 32 in 32..1024"};
+  if (o.ctas_per_sm > 8) throw ArgError{"ctas_per_sm must be 0..8"};
   CK(cudaSetDevice(device));
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : stream;
   has_results = false;
@@ -87,44 +268,12 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (W_pad > (1ull << 31) || tiles * (uint64_t)N * kTileWords > (1ull << 40))
     throw LimitError{"pattern block too large"};
 
-  // Sweep shape: M words per item (the largest whose slots fit in shared
-  // memory), a schedule for residue groups of 16/M, two record staging
-  // buffers in the rest, and the CTA size.
-  const size_t static_smem = 256;
-  const size_t budget = smem_optin > static_smem + 1024 ? smem_optin - static_smem - 1024 : 0;
-  int M = (int)o.words_per_item;
-  const bool fixed_M = M != 0;
-  if (!M) {
-    M = 8;
-    while (M > 1 && (size_t)plan.max_live * M * 8 > budget) M /= 2;
-  }
-  for (;;) {
-    if (sched_M != M) {
-      build_schedule(nl, plan, 16u / (uint32_t)M, sched);
-      sched_M = M;
-      sched_uploaded = false;
-    }
-    const bool fits = sched.max_live <= kMaxSlots && (size_t)sched.max_live * M * 8 <= budget;
-    if (fits) break;
-    if (fixed_M || M == 1)
-      throw LimitError{"a sweep needs " + std::to_string(sched.max_live) +
-                       " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
-                       " at " + std::to_string(M) + " word(s) per item"};
-    M /= 2;
-  }
-  const size_t vals_bytes = ((size_t)sched.max_live * M * 8 + 15) / 16 * 16;
   uint32_t widest = 1;
   std::vector<uint32_t> widths;
   for (uint32_t l = 1; l <= plan.max_gate_level && l < plan.n_levels; ++l) {
     widths.push_back(plan.level_off[l + 1] - plan.level_off[l]);
     widest = std::max(widest, widths.back());
   }
-  const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (budget - vals_bytes) / 32);
-  const size_t smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
-  const uint32_t tmax = sweep_max_threads(M);
-  int threads = o.block_threads ? (int)o.block_threads : (int)pick_sweep_threads(widths, M);
-  threads = std::min<int>(threads, (int)tmax);
-
   cudaEvent_t e0 = ev(0), e1 = ev(1), e2 = ev(2), e3 = ev(3);
   CK(cudaEventRecord(e0, s));
   if (!plan_uploaded) {
@@ -139,12 +288,6 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     upload(d_inj, plan.sweeps, s);
     upload(d_exact, plan.exact_fault, s);
     plan_uploaded = true;
-  }
-  if (!sched_uploaded) {
-    upload(d_recs, sched.recs, s);
-    upload(d_li_off, sched.li_off, s);
-    upload(d_li, sched.li, s);
-    sched_uploaded = true;
   }
   if (!pats_uploaded) {
     upload(d_pwords, pats.words, s);
@@ -166,6 +309,57 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     d_exact_list[0].ensure(std::max<uint32_t>(n_exact, 1) * 4);
     d_exact_list[1].ensure(std::max<uint32_t>(n_exact, 1) * 4);
     d_nout.ensure(16);
+  }
+
+  // Sweep shape: explicit options, the autotuned shape of this plan, or the
+  // default (the largest words per item that fits; two CTAs per SM when 8
+  // or 4 words per item leave room for them).
+  double tune_ms_now = 0;
+  int M = 0, occ = 1, threads = 0;
+  const bool explicit_shape = o.words_per_item || o.block_threads || o.ctas_per_sm;
+  if (explicit_shape) {
+    M = (int)o.words_per_item;
+    occ = o.ctas_per_sm ? (int)o.ctas_per_sm : 1;
+    threads = (int)o.block_threads;
+  } else if (o.tune && n_sweeps && tiles) {
+    if (tuned_gen != plan_gen) {
+      const auto t0 = std::chrono::steady_clock::now();
+      tune_shape(s, widths, widest);
+      tune_ms_now = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    M = tuned_M;
+    occ = tuned_occ;
+    threads = tuned_T;
+  } else {
+    default_shape(widths, widest, M, occ, threads);
+  }
+  const size_t budget = sweep_smem_share(smem_optin, smem_per_sm, occ);
+  const bool fixed_M = M != 0;
+  if (!M) {
+    M = 8;
+    while (M > 1 && sweep_vals_bytes(plan.max_live, M) > budget) M /= 2;
+  }
+  for (;;) {
+    use_schedule(M);
+    const bool fits = sched.max_live <= kMaxSlots && sweep_vals_bytes(sched.max_live, M) <= budget;
+    if (fits) break;
+    if (fixed_M || M == 1)
+      throw LimitError{"a sweep needs " + std::to_string(sched.max_live) +
+                       " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
+                       " at " + std::to_string(M) + " word(s) per item and " + std::to_string(occ) +
+                       " CTA(s) per SM"};
+    M /= 2;
+  }
+  const size_t vals_bytes = sweep_vals_bytes(sched.max_live, M);
+  const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (budget - vals_bytes) / 32);
+  const size_t smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
+  if (!threads) threads = (int)pick_sweep_threads(widths, M);
+  threads = std::min<int>(threads, (int)sweep_max_threads(M));
+  if (!sched_uploaded) {
+    upload(d_recs, sched.recs, s);
+    upload(d_li_off, sched.li_off, s);
+    upload(d_li, sched.li, s);
+    sched_uploaded = true;
   }
   CK(cudaMemsetAsync(d_queue.p, 0, std::max<uint64_t>(tiles, 1) * sizeof(int), s));
   CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
@@ -196,10 +390,10 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   CK(cudaEventRecord(e2, s));
 
   CK(sweep_set_smem(M, smem));
-  int occ = 0;
-  CK(sweep_occupancy(M, threads, smem, &occ));
-  if (occ < 1) throw LimitError{"sweep kernel does not fit on an SM with this shape"};
-  const int blocks = n_sms * occ;
+  int occ_got = 0;
+  CK(sweep_occupancy(M, threads, smem, &occ_got));
+  if (occ_got < 1) throw LimitError{"sweep kernel does not fit on an SM with this shape"};
+  const int blocks = n_sms * occ_got;
 
   // 3. tiles
   uint32_t n_sw = n_sweeps, n_rt = n_roots, n_ex = n_exact;
@@ -409,6 +603,8 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   stats.max_live = sched.max_live;
   stats.bank_conflict_groups = sched.conflict_groups;
   stats.bank_access_groups = sched.access_groups;
+  stats.ms_tune = tune_ms_now;
+  stats.ctas_per_sm = (uint32_t)occ_got;
   stats.words_per_item = (uint32_t)M;
   stats.block_threads = (uint32_t)threads;
   stats.blocks = (uint32_t)blocks;
@@ -441,9 +637,12 @@ int fsimb_create(int device, fsimb_handle** out) {
       int sms = 0, optin = 0;
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
       CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+      int per_sm = 0;
+      CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
       h->device = device;
       h->n_sms = sms;
       h->smem_optin = (size_t)optin;
+      h->smem_per_sm = (size_t)per_sm;
       CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     }
   } catch (const CudaError& e) {
@@ -510,7 +709,7 @@ int fsimb_set_faults(fsimb_handle* h, const uint32_t* site, const uint8_t* pin,
   }
   h->faults = std::move(fs);
   h->has_faults = true;
-  h->gen = next_generation();
+  h->gen = h->plan_gen = next_generation();
   h->plan_valid = false;
   h->plan_uploaded = false;
   h->has_results = false;

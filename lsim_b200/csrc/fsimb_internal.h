@@ -103,6 +103,22 @@ inline uint32_t pick_sweep_threads(std::vector<uint32_t>& widths, int M) {
   return best;
 }
 
+// Dynamic shared memory one sweep CTA may take when `occ` CTAs share an SM
+// (each CTA also holds the kernel's static __shared__ variables and the
+// 1 KB the hardware reserves per CTA).
+inline size_t sweep_smem_share(size_t smem_optin, size_t smem_per_sm, int occ) {
+  const size_t static_smem = 512, reserved = 1024;
+  const size_t budget = smem_optin > static_smem + reserved ? smem_optin - static_smem - reserved : 0;
+  if (occ <= 1) return budget;
+  const size_t per = smem_per_sm / (size_t)occ;
+  return per > static_smem + reserved ? std::min(budget, per - static_smem - reserved) : 0;
+}
+
+// Bytes of a sweep CTA's value slots: max_live slots of M words, 16-byte rounded.
+inline uint32_t sweep_vals_bytes(uint32_t max_live, int M) {
+  return (uint32_t)(((size_t)max_live * M * 8 + 15) / 16 * 16);
+}
+
 // Page-locked host staging buffer.
 struct PinnedBuf {
   void* p = nullptr;
@@ -139,10 +155,11 @@ uint64_t next_generation();
 struct fsimb_handle {
   int device = -1;
   int n_sms = 0;
-  size_t smem_optin = 0;
+  size_t smem_optin = 0, smem_per_sm = 0;
   cudaStream_t stream = nullptr;
   std::string err;
-  uint64_t gen = 0;  // changes whenever circuit, faults or patterns change
+  uint64_t gen = 0;       // changes whenever circuit, faults or patterns change
+  uint64_t plan_gen = 0;  // changes whenever circuit or faults change
 
   fsimb::Netlist nl;
   bool has_ckt = false;
@@ -157,11 +174,18 @@ struct fsimb_handle {
   fsimb::Schedule sched;          // for sched_M words per item
   int sched_M = 0;
   bool sched_uploaded = false;
+  // Schedules built so far for this plan, per words per item (1, 2, 4, 8).
+  fsimb::Schedule sched_cache[4];
+  uint64_t sched_cache_gen[4] = {0, 0, 0, 0};
+  // Autotuned sweep shape of plan_gen (fsimb_opts.tune).
+  uint64_t tuned_gen = 0;
+  int tuned_M = 0, tuned_T = 0, tuned_occ = 0;
+  cudaEvent_t tune_ev[2] = {nullptr, nullptr};
 
   fsimb::DevBuf d_type, d_fi_off, d_fi_idx, d_recs, d_level, d_level_off, d_li_off, d_li;
   fsimb::DevBuf d_roots, d_members, d_traced, d_inj, d_exact;
   fsimb::DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue, d_err;
-  fsimb::DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout;
+  fsimb::DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout, d_tune_list;
   uint64_t good_tiles = 0;  // tiles held in d_good
   uint64_t good_P = 0;
   bool pats_uploaded = false;  // d_pwords holds the current patterns
@@ -178,9 +202,11 @@ struct fsimb_handle {
                         &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                         &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
                         &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
-                        &d_exact_list[0], &d_exact_list[1], &d_nout})
+                        &d_exact_list[0], &d_exact_list[1], &d_nout, &d_tune_list})
         b->release();
       for (auto e : events) cudaEventDestroy(e);
+      for (auto e : tune_ev)
+        if (e) cudaEventDestroy(e);
       if (stream) cudaStreamDestroy(stream);
     }
   }
@@ -200,7 +226,7 @@ struct fsimb_handle {
                             &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                             &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
                             &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
-                            &d_exact_list[0], &d_exact_list[1], &d_nout})
+                            &d_exact_list[0], &d_exact_list[1], &d_nout, &d_tune_list})
       s += b->n;
     return s;
   }
@@ -221,7 +247,7 @@ struct fsimb_handle {
     fsimb::parse_ckt(t, n, tmp);
     nl = std::move(tmp);
     has_ckt = true;
-    gen = fsimb::next_generation();
+    gen = plan_gen = fsimb::next_generation();
     invalidate_circuit();
     faults.clear();
     pats = fsimb::Patterns();
@@ -232,7 +258,7 @@ struct fsimb_handle {
     fsimb::parse_flst(t, n, nl, tmp);
     faults = std::move(tmp);
     has_faults = true;
-    gen = fsimb::next_generation();
+    gen = plan_gen = fsimb::next_generation();
     plan_valid = false;
     plan_uploaded = false;
     has_results = false;
@@ -250,6 +276,16 @@ struct fsimb_handle {
   }
 
   void run(const fsimb_opts* opts);
+  // The schedule at M words per item for the current plan (cached per M).
+  const fsimb::Schedule& cached_schedule(int M);
+  // Makes `sched` the schedule at M (re-uploaded before the next sweep).
+  void use_schedule(int M);
+  // Default sweep shape; M = 0 / threads = 0 leave the choice to run().
+  void default_shape(std::vector<uint32_t> widths, uint32_t widest, int& M, int& occ, int& threads);
+  // Times candidate shapes on a strided sample of tile 0's sweeps and keeps
+  // the fastest in tuned_M / tuned_T / tuned_occ.  Needs the plan and the
+  // patterns on the device.
+  void tune_shape(cudaStream_t s, const std::vector<uint32_t>& widths, uint32_t widest);
 };
 
 // Wraps a C ABI body: exceptions become status codes and (h)->err.

@@ -450,42 +450,58 @@ __global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(
 }
 
 // Batch form: items of many circuits of one shape class, in circuit order;
-// each item names (circuit, tile, sweep, subtile).
+// each item names (circuit, tile, sweep, subtile).  A CTA's items come in
+// increasing order, so it keeps the current circuit's item range and
+// descriptor in shared memory and looks a circuit up only when it moves on.
 template <int M>
-__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep_batch(BatchSweepArgs a) {
+__global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64)) k_sweep_batch(BatchSweepArgs a) {
   extern __shared__ __align__(16) uint64_t vals[];
   __shared__ unsigned long long acc[M];
   __shared__ __align__(8) uint64_t bars[2];
-  __shared__ unsigned long long s_item, s_local;
-  __shared__ uint32_t s_circ;
+  __shared__ unsigned long long s_item, s_lo, s_hi;
+  __shared__ uint32_t s_cidx, s_new;
+  __shared__ __align__(16) BatchCirc s_c;
   SweepCta k;
   sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc);
+  if (threadIdx.x == 0) {
+    s_lo = 0;
+    s_hi = 0;
+  }
   const uint32_t subtiles = kTileWords / M;
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned long long it = atomicAdd(a.queue, 1ull);
       s_item = it;
-      if (it < a.n_items) {  // circuit holding the item: last prefix <= it
+      s_new = 0;
+      if (it < a.n_items && (it < s_lo || it >= s_hi)) {  // last prefix <= it
         const uint32_t lo = find_prefix(a.item_prefix, a.n_circ, it);
-        s_circ = a.circ_ids[lo];
-        s_local = it - a.item_prefix[lo];
+        s_lo = a.item_prefix[lo];
+        s_hi = lo + 1 < a.n_circ ? a.item_prefix[lo + 1] : a.n_items;
+        s_cidx = a.circ_ids[lo];
+        s_new = 1;
       }
     }
     __syncthreads();
     const unsigned long long item = s_item;
-    const uint32_t ci = s_circ;
-    const unsigned long long local = s_local;
-    __syncthreads();
     if (item >= a.n_items) return;
-    const BatchCirc& c = a.circs[ci];
-    const uint64_t per_tile = (uint64_t)c.n_sweeps * subtiles;
+    if (s_new) {
+      constexpr int nw = sizeof(BatchCirc) / 8;
+      static_assert(sizeof(BatchCirc) % 8 == 0, "BatchCirc is copied as 8-byte words");
+      if (threadIdx.x < nw)
+        reinterpret_cast<unsigned long long*>(&s_c)[threadIdx.x] =
+            reinterpret_cast<const unsigned long long*>(a.circs + s_cidx)[threadIdx.x];
+      __syncthreads();
+    }
+    // s_item / s_lo / s_c are rewritten only after sweep_item's barriers.
+    const unsigned long long local = item - s_lo;
+    const uint64_t per_tile = (uint64_t)s_c.n_sweeps * subtiles;
     const uint32_t tile = (uint32_t)(local / per_tile);
     const uint64_t rem = local % per_tile;
     const uint32_t si = (uint32_t)(rem / subtiles);
     const uint32_t w0 = (uint32_t)(rem % subtiles) * M;
-    const SweepView v{c.recs, c.level, c.level_off, c.li_off, c.li, c.fi_off, c.fi_idx, c.type,
-                      c.good + (uint64_t)tile * c.N * 32, c.max_gate_level};
-    if (!sweep_item<M>(k, v, c.inj[si], w0, c.out + ((uint64_t)tile * c.n_sweeps + si) * 32)) {
+    const SweepView v{s_c.recs, s_c.level, s_c.level_off, s_c.li_off, s_c.li, s_c.fi_off, s_c.fi_idx,
+                      s_c.type, s_c.good + (uint64_t)tile * s_c.N * 32, s_c.max_gate_level};
+    if (!sweep_item<M>(k, v, s_c.inj[si], w0, s_c.out + ((uint64_t)tile * s_c.n_sweeps + si) * 32)) {
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       return;
     }

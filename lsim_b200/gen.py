@@ -15,6 +15,10 @@ from the previous level; POs are driven by sink gates of the top levels.
   c3  2,000,000 gates, 5,000 PI / 5,000 PO, 400 levels, 10% of gates with a
       fanout target of 8-64 (the rest 1-3), output + input-pin faults
       collapsed, 16,384 patterns with half of the PIs at P(1) = 0.2.
+
+``batch_configs`` draws the batched configuration (c4): circuits with gate
+counts log-uniform in 500-50,000, 10-120 levels, SA0/SA1 on every gate
+output and 1,024-16,384 uniform patterns each.
 """
 import ctypes
 
@@ -83,3 +87,25 @@ def workload(name, **overrides):
     cfg = dict(WORKLOADS[name])
     cfg.update(overrides)
     return generate(**cfg)
+
+
+def batch_configs(n_circuits=256, seed=0, gates=(500, 50000), levels=(10, 120),
+                  patterns=(1024, 16384), faults="outputs", type_mask=BENCH_TYPES):
+    """Per-circuit ``generate`` arguments of a batch, drawn from ``seed``.
+
+    Gate counts are log-uniform in ``gates``, levels uniform in ``levels``
+    (at most a quarter of the gate count), pattern counts uniform in
+    ``patterns``; PIs and POs are a 32nd of the gates, 16-1,000."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_circuits):
+        g = int(round(np.exp(rng.uniform(np.log(gates[0]), np.log(gates[1])))))
+        lv = int(rng.integers(levels[0], levels[1] + 1))
+        lv = max(2, min(lv, g // 4))
+        io = int(min(1000, max(16, g // 32)))
+        P = int(rng.integers(patterns[0], patterns[1] + 1))
+        out.append(dict(n_gates=g, n_pi=io, n_po=io, n_levels=lv, p_fanin3=0.5,
+                        seed=seed * 100003 + i + 1, n_patterns=P, faults=faults,
+                        type_mask=type_mask))
+    return out

@@ -110,9 +110,9 @@ class Simulator:
 
     # ------------------------------------------------------------ running
     def run(self, mode=Mode.CUDA_B200, num_threads=1, drop=False, words_per_item=0,
-            block_threads=0, stream=None):
+            block_threads=0, ctas_per_sm=0, tune=False, stream=None):
         o = _lib.Opts(ctypes.sizeof(_lib.Opts), 1 if drop else 0, words_per_item, block_threads,
-                      stream)
+                      ctas_per_sm, 1 if tune else 0, stream)
         self._check(_lib.lib().fsimb_run(self._h, ctypes.byref(o)))
         self._ran = True
 

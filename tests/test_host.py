@@ -166,3 +166,25 @@ def test_dot_matches_reference_visualization(basics):
         sim = Simulator(-1)
         sim.read_text(c["ckt"], c["flst"], c["ptn"])
         assert sim.dot() == d["dot"], c["name"]
+
+
+def test_batch_needs_a_gpu():
+    """No CPU fallback: creating a batch without a usable device fails loudly."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from lsim_b200 import Batch
+    with pytest.raises(FsimbError) as e:
+        Batch(0)
+    assert e.value.code == _lib.ERR_CUDA
+
+
+def test_batch_configs_follow_the_batched_configuration():
+    cfgs = gen.batch_configs(256, seed=0)
+    assert len(cfgs) == 256
+    g = np.array([c["n_gates"] for c in cfgs])
+    assert g.min() >= 500 and g.max() <= 50000
+    assert np.median(g) < 10000  # log-uniform, not uniform
+    assert all(10 <= c["n_levels"] <= 120 for c in cfgs)
+    assert all(1024 <= c["n_patterns"] <= 16384 for c in cfgs)
+    assert cfgs == gen.batch_configs(256, seed=0)
