@@ -252,6 +252,8 @@ typedef struct {
   double ms_sweep;           /* the class's launch, when run without the graph */
 } fsimb_batch_class;
 int fsimb_batch_class_stats(const fsimb_batch* b, uint32_t index, fsimb_batch_class* out);
+/* Member indices (order of fsimb_batch_add) of a class; n >= its n_circuits. */
+int fsimb_batch_class_members(const fsimb_batch* b, uint32_t index, uint32_t* out, uint64_t n);
 
 /* Synthetic workloads (seeded; text in LSIM's formats).  Returned buffers
  * are released with fsimb_free_text. */

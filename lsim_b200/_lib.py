@@ -158,6 +158,7 @@ SIGNATURES = {
     "fsimb_batch_run": (ctypes.c_int, [_P, ctypes.POINTER(BatchOpts)]),
     "fsimb_batch_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
     "fsimb_batch_class_stats": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(BatchClass)]),
+    "fsimb_batch_class_members": (ctypes.c_int, [_P, ctypes.c_uint32, _U32P, _U64]),
 }
 
 _lib = None

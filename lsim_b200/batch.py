@@ -74,7 +74,11 @@ class Batch:
             c = _lib.BatchClass()
             if _lib.lib().fsimb_batch_class_stats(self._b, i, ctypes.byref(c)) != 0:
                 return out
-            out.append(c.as_dict())
+            d = c.as_dict()
+            ids = (ctypes.c_uint32 * max(1, c.n_circuits))()
+            self._check(_lib.lib().fsimb_batch_class_members(self._b, i, ids, c.n_circuits))
+            d["members"] = list(ids)[:c.n_circuits]
+            out.append(d)
             i += 1
 
     @property

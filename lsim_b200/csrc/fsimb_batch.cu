@@ -269,6 +269,7 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
 
   // Sweep classes: shapes[c] runs the jobs with cls == c.
   classes.clear();
+  uint32_t n_counters = 0;
   for (int a = 0; a < 4; ++a) smem_attr[a] = 0;
   for (size_t ci = 0; ci < shapes.size(); ++ci) {
     const ClassShape& sh = shapes[ci];
@@ -280,9 +281,12 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
     for (size_t i = 0; i < n; ++i) {
       if (jobs[i].cls != (int)ci || circs[i].n_sweeps == 0) continue;
       if (jobs[i].M != sh.M) throw ArgError{"batch job's words per item differ from its class"};
+      const unsigned long long ci_items =
+          (unsigned long long)circs[i].tiles * circs[i].n_sweeps * (kTileWords / sh.M);
+      if (ci_items >= 0xFFFFFFFFull)
+        throw LimitError{"a batch circuit has 2^32 or more sweep items; run it on its own"};
       k.circ_ids.push_back((uint32_t)i);
-      k.item_prefix.push_back(items);
-      items += (unsigned long long)circs[i].tiles * circs[i].n_sweeps * (kTileWords / sh.M);
+      items += ci_items;
       k.work += (double)jobs[i].plan->dense_sweep_gates * circs[i].tiles;
       max_live = std::max(max_live, jobs[i].sched->max_live);
       const Plan& p = *jobs[i].plan;
@@ -293,6 +297,8 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
     k.n_items = items;
     k.max_live = max_live;
     k.widest = widest;
+    k.queue_base = n_counters;
+    n_counters += (uint32_t)k.circ_ids.size();
     size_class(k, sh);
     classes.push_back(std::move(k));
   }
@@ -310,7 +316,6 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
   // Descriptor block: circuits, good segments, class tables, unit prefixes.
   uint64_t dsz = align256(n * sizeof(BatchCirc)) + align256(segs.size() * sizeof(BatchGoodSeg)) +
                  2 * align256((n + 1) * 8);
-  for (const SweepClass& k : classes) dsz += align256(k.circ_ids.size() * 4) + align256(k.item_prefix.size() * 8);
   d_desc.ensure(dsz);
   h_desc.ensure(dsz);
   {
@@ -327,15 +332,11 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
     dd_segs = (const BatchGoodSeg*)put(segs.data(), segs.size() * sizeof(BatchGoodSeg));
     dd_ffr_prefix = (const unsigned long long*)put(ffr_prefix.data(), (n + 1) * 8);
     dd_exact_prefix = (const unsigned long long*)put(exact_prefix.data(), (n + 1) * 8);
-    for (SweepClass& k : classes) {
-      k.dd_circ_ids = (const uint32_t*)put(k.circ_ids.data(), k.circ_ids.size() * 4);
-      k.dd_item_prefix = (const unsigned long long*)put(k.item_prefix.data(), k.item_prefix.size() * 8);
-    }
     CK(cudaMemcpyAsync(d_desc.p, h_desc.p, at, cudaMemcpyHostToDevice, s));
     desc_bytes = at;
   }
   // Control words: one work counter per class and the error flag.
-  ctl_bytes = align256((classes.size() + 1) * 8);
+  ctl_bytes = align256(((uint64_t)n_counters + 1) * 8);
   d_ctl.ensure(ctl_bytes);
   h_res.ensure(std::max<uint64_t>(F_total, 1) * 17 + 64);
   n_circ = (uint32_t)n;
@@ -371,10 +372,6 @@ void BatchExec::relaunch_shapes(const std::vector<ClassShape>& shapes) {
     size_class(k, sh);
   }
   invalidate_graph();
-}
-
-void BatchExec::reset_attributes() {
-  for (int a = 0; a < 4; ++a) smem_attr[a] = 0;
 }
 
 void BatchExec::apply_attributes() {
@@ -460,18 +457,39 @@ uint64_t BatchExec::enqueue_sweeps(cudaStream_t s, int only) {
   for (size_t ci = 0; ci < classes.size(); ++ci) {
     const SweepClass& k = classes[ci];
     if (only >= 0 && k.id != only) continue;
-    BatchSweepArgs a{};
-    a.circs = dd_circs;
-    a.circ_ids = k.dd_circ_ids;
-    a.item_prefix = k.dd_item_prefix;
-    a.n_circ = (uint32_t)k.circ_ids.size();
-    a.n_items = k.n_items;
-    a.queue = d_ctl.as<unsigned long long>() + 1 + ci;
-    a.vals_bytes = k.vals_bytes;
-    a.rec_buf = k.rec_buf;
-    a.err = d_ctl.as<int>();
-    CK(launch_sweep_batch(k.shape.M, k.threads, k.blocks, k.smem, a, s));
-    ++launches;
+    // one launch per kSweepCircsPerLaunch circuits of the class
+    for (size_t j0 = 0; j0 < k.circ_ids.size(); j0 += kSweepCircsPerLaunch) {
+      const size_t j1 = std::min(k.circ_ids.size(), j0 + (size_t)kSweepCircsPerLaunch);
+      params.n_circ = (uint32_t)(j1 - j0);
+      unsigned long long chunk_items = 0;
+      for (size_t j = j0; j < j1; ++j) {
+        const BatchCirc& c = circs[k.circ_ids[j]];
+        SweepCirc& d = params.c[j - j0];
+        d.recs = c.recs;
+        d.level = c.level;
+        d.level_off = c.level_off;
+        d.li_off = c.li_off;
+        d.li = c.li;
+        d.fi_off = c.fi_off;
+        d.fi_idx = c.fi_idx;
+        d.type = c.type;
+        d.inj = c.inj;
+        d.good = c.good;
+        d.out = c.out;
+        d.N = c.N;
+        d.n_sweeps = c.n_sweeps;
+        d.max_gate_level = c.max_gate_level;
+        d.n_items = c.tiles * c.n_sweeps * (kTileWords / (uint32_t)k.shape.M);
+        chunk_items += d.n_items;
+      }
+      params.queue = d_ctl.as<unsigned long long>() + 1 + k.queue_base + j0;
+      params.err = d_ctl.as<int>();
+      params.vals_bytes = k.vals_bytes;
+      params.rec_buf = k.rec_buf;
+      const int blocks = (int)std::min<unsigned long long>((unsigned long long)k.blocks, chunk_items);
+      CK(launch_sweep_batch(k.shape.M, k.threads, std::max(blocks, 1), k.smem, params, s));
+      ++launches;
+    }
   }
   return launches;
 }
@@ -563,6 +581,7 @@ bool same_shapes(const std::vector<ClassShape>& a, const std::vector<ClassShape>
 struct BatchAssign {
   std::vector<int> M, cls;
   std::vector<ClassShape> shapes;
+  std::vector<uint32_t> max_live;  // per class: the largest member schedule's slots
 };
 
 struct fsimb_batch {
@@ -649,15 +668,8 @@ struct fsimb_batch {
   std::vector<int> schedules(int M, size_t share) {
     std::vector<int> got(members.size(), 0);
     parallel_for(members.size(), [&](size_t i) {
-      fsimb_handle* h = members[i];
       for (int m = M; m >= 1; m /= 2) {
-        MemberCache& c = cache[i];
-        const int sl = m_slot(m);
-        if (!c.has[sl]) {
-          build_schedule(h->nl, h->plan, 16u / (uint32_t)m, c.sched[sl]);
-          c.has[sl] = true;
-        }
-        const Schedule& sc = c.sched[sl];
+        const Schedule& sc = schedule_at(i, m);
         if (sc.max_live <= kMaxSlots && sweep_vals_bytes(sc.max_live, m) <= share) {
           got[i] = m;
           return;
@@ -677,34 +689,42 @@ struct fsimb_batch {
       widths.push_back(p.level_off[l + 1] - p.level_off[l]);
   }
 
-  // Automatic classes: each member at the shape the plain path would give it
-  // alone -- the largest words per item that fits, the CTA size from its
-  // level widths, and the CTAs per SM its own shared memory and registers
-  // allow -- and members of the same shape share a class.  A class's shared
-  // memory is capped at the share of its CTAs per SM, so no member runs at a
-  // lower occupancy than alone.
+  // Automatic classes: each member at the default shape the plain path would
+  // give it alone (default_sweep_shape, with the batch kernel's occupancy),
+  // and members of the same shape share a class.  A class's shared memory is
+  // capped at the share of its CTAs per SM, so no member runs at a lower
+  // occupancy than alone.
   BatchAssign auto_assign() {
     BatchAssign a;
-    const size_t budget = smem_share(1);
-    a.M = schedules(8, budget);
     const size_t n = members.size();
-    for (int M : {1, 2, 4, 8}) CK(sweep_batch_set_smem(M, budget));
-    exec.reset_attributes();
+    a.M.resize(n);
     std::vector<ClassShape> shape(n);
     std::vector<long long> key(n);
+    const size_t share2 = smem_share(2);
+    parallel_for(n, [&](size_t i) {  // the schedules the default shape looks at first
+      for (int m : {8, 4})
+        if (sweep_vals_bytes(members[i]->plan.max_live, m) <= share2) schedule_at(i, m);
+    });
     for (size_t i = 0; i < n; ++i) {
       std::vector<uint32_t> w;
       level_widths(i, w);
       uint32_t widest = 1;
       for (uint32_t x : w) widest = std::max(widest, x);
-      const int M = a.M[i];
-      const uint32_t t = pick_sweep_threads(w, M);
-      const uint32_t vals = sweep_vals_bytes(cache[i].sched[m_slot(M)].max_live, M);
-      const size_t smem = std::max<size_t>(16, vals + std::min<size_t>(widest, (budget - vals) / 32) * 32);
-      int occ = 0;
-      CK(sweep_batch_occupancy(M, (int)t, smem, &occ));
-      occ = std::max(1, std::min(occ, 16));
-      shape[i] = ClassShape{M, (int)t, occ};
+      int M = 0, occ = 1, t = 0;
+      default_sweep_shape(
+          members[i]->plan, [&](int m) -> const Schedule& { return schedule_at(i, m); },
+          [&](int m, int th, size_t smem) {
+            CK(sweep_batch_set_smem(m, smem));
+            int got = 0;
+            CK(sweep_batch_occupancy(m, th, smem, &got));
+            return got;
+          },
+          std::move(w), widest, smem_optin, smem_per_sm, M, occ, t);
+      if (sweep_vals_bytes(schedule_at(i, M).max_live, M) > smem_share(occ))
+        throw LimitError{"batch member " + std::to_string(i) +
+                         " has more live values than shared memory holds at 1 word per item"};
+      a.M[i] = M;
+      shape[i] = ClassShape{M, t, occ};
       key[i] = ((long long)m_slot(M) * 4096 + t) * 32 + occ;
     }
     std::vector<long long> keys(key);
@@ -712,11 +732,25 @@ struct fsimb_batch {
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     a.cls.resize(n);
     a.shapes.resize(keys.size());
+    a.max_live.assign(keys.size(), 0);
     for (size_t i = 0; i < n; ++i) {
-      a.cls[i] = (int)(std::lower_bound(keys.begin(), keys.end(), key[i]) - keys.begin());
-      a.shapes[a.cls[i]] = shape[i];
+      const int c = (int)(std::lower_bound(keys.begin(), keys.end(), key[i]) - keys.begin());
+      a.cls[i] = c;
+      a.shapes[c] = shape[i];
+      a.max_live[c] = std::max(a.max_live[c], schedule_at(i, a.M[i]).max_live);
     }
     return a;
+  }
+
+  // The member's schedule at M words per item (built once per plan).
+  const Schedule& schedule_at(size_t i, int m) {
+    MemberCache& c = cache[i];
+    const int sl = m_slot(m);
+    if (!c.has[sl]) {
+      build_schedule(members[i]->nl, members[i]->plan, 16u / (uint32_t)m, c.sched[sl]);
+      c.has[sl] = true;
+    }
+    return c.sched[sl];
   }
 
   // Explicit shape: every member at words_per_item (or the largest smaller
@@ -757,8 +791,9 @@ struct fsimb_batch {
     return js;
   }
 
-  // Times candidate CTA sizes per class on the first tile of a spread of the
-  // class's circuits (about 3% of its sweep work) and keeps the fastest.
+  // Times candidate shapes per class (CTAs per SM x CTA size, words per item
+  // fixed) on the first tile of a spread of the class's circuits (about 3%
+  // of its sweep work); the default shape stays unless beaten by 2%.
   void autotune(BatchAssign& a, cudaStream_t s) {
     const size_t n = members.size();
     const size_t n_cls = a.shapes.size();
@@ -796,38 +831,56 @@ struct fsimb_batch {
     cudaEvent_t e0 = ev(0), e1 = ev(1);
     std::vector<ClassShape> cur = a.shapes;
     for (size_t c = 0; c < n_cls; ++c) {
-      bool present = false;
-      for (const SweepClass& k : tx.classes) present |= k.id == (int)c;
-      if (!present) continue;
-      const int M = a.shapes[c].M;
-      const int tmax = (int)sweep_max_threads(M);
-      const int base = a.shapes[c].threads;
-      std::vector<int> cands;
-      for (int t : {base / 2, base, base * 2, base * 4}) {
-        t = std::max(64, std::min(tmax, (t + 31) / 32 * 32));
-        if (std::find(cands.begin(), cands.end(), t) == cands.end()) cands.push_back(t);
-      }
+      SweepClass* kc = nullptr;
+      for (SweepClass& k : tx.classes)
+        if (k.id == (int)c) kc = &k;
+      if (!kc) continue;  // no sampled circuit in this class
+      const ClassShape def = a.shapes[c];
+      const int M = def.M;
+      std::vector<ClassShape> cands{def};
+      for (int occ : {1, 2, 3, 4})
+        for (int T : {128, 256, 384, 512, 768, 1024})
+          if (T <= (int)sweep_max_threads(M) && T * occ <= 2048 && !(occ == def.occ && T == def.threads))
+            cands.push_back(ClassShape{M, T, occ});
       float best_ms = 1e30f;
-      int best_t = base;
-      for (int t : cands) {
-        cur[c].threads = t;
-        tx.relaunch_shapes(cur);
-        CK(cudaMemsetAsync(tx.d_ctl.p, 0, tx.ctl_bytes, s));
-        CK(cudaEventRecord(e0, s));
-        tx.enqueue_sweeps(s, (int)c);
-        CK(cudaEventRecord(e1, s));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        int kerr = 0;
-        CK(cudaMemcpy(&kerr, tx.d_ctl.p, sizeof(int), cudaMemcpyDeviceToHost));
-        if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
-        if (ms < best_ms) {
+      ClassShape best = def;
+      bool best_is_default = false;
+      for (const ClassShape& sh : cands) {
+        // every member of the class, not only the sampled ones, must fit
+        if (sweep_vals_bytes(a.max_live[c], M) > smem_share(sh.occ)) continue;
+        try {
+          tx.size_class(*kc, sh);
+        } catch (const LimitError&) {
+          continue;  // slots do not fit this many CTAs per SM
+        }
+        if (kc->blocks < (int)std::min<unsigned long long>((unsigned long long)n_sms * sh.occ, kc->n_items))
+          continue;  // fewer CTAs per SM than asked: the same as a smaller shape
+        // an untimed run of the first candidate warms the GPU up; then the
+        // fastest of two timed runs counts
+        float ms = 1e30f;
+        for (int rep = (&sh == &cands[0]) ? -1 : 0; rep < 2; ++rep) {
+          CK(cudaMemsetAsync(tx.d_ctl.p, 0, tx.ctl_bytes, s));
+          CK(cudaEventRecord(e0, s));
+          tx.enqueue_sweeps(s, (int)c);
+          CK(cudaEventRecord(e1, s));
+          CK(cudaEventSynchronize(e1));
+          float x = 0;
+          CK(cudaEventElapsedTime(&x, e0, e1));
+          int kerr = 0;
+          CK(cudaMemcpy(&kerr, tx.d_ctl.p, sizeof(int), cudaMemcpyDeviceToHost));
+          if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
+          if (rep >= 0) ms = std::min(ms, x);
+        }
+        // the default shape stays unless a candidate beats it by 2%
+        const bool is_default = sh.occ == def.occ && sh.threads == def.threads;
+        if (is_default || ms < (best_is_default ? 0.98f : 1.0f) * best_ms) {
           best_ms = ms;
-          best_t = t;
+          best = sh;
+          best_is_default = is_default;
         }
       }
-      cur[c].threads = best_t;
+      tx.size_class(*kc, best);
+      cur[c] = best;
     }
     a.shapes = cur;
     tx.release();
@@ -1084,6 +1137,15 @@ int fsimb_batch_class_stats(const fsimb_batch* b, uint32_t i, fsimb_batch_class*
   out->max_live = k.max_live;
   out->widest_level = k.widest;
   out->ms_sweep = i < b->class_ms.size() ? b->class_ms[i] : 0.0;
+  return FSIMB_OK;
+}
+
+int fsimb_batch_class_members(const fsimb_batch* b, uint32_t i, uint32_t* out, uint64_t n) {
+  if (!b) return FSIMB_ERR_ARG;
+  if (i >= b->exec.classes.size()) return FSIMB_ERR_ARG;
+  const SweepClass& k = b->exec.classes[i];
+  if (n < k.circ_ids.size() || (!out && !k.circ_ids.empty())) return FSIMB_ERR_ARG;
+  std::copy(k.circ_ids.begin(), k.circ_ids.end(), out);
   return FSIMB_OK;
 }
 

@@ -38,8 +38,8 @@ struct BatchJob {
 struct SweepClass {
   int id = 0;  // index into the layout's shapes
   ClassShape shape{0, 0, 0};
-  std::vector<uint32_t> circ_ids;
-  std::vector<unsigned long long> item_prefix;
+  std::vector<uint32_t> circ_ids;   // members, in launch order
+  uint32_t queue_base = 0;          // their work counters: d_ctl words 1 + queue_base + j
   unsigned long long n_items = 0;
   double work = 0;        // gate-words its sweeps evaluate (launch order)
   uint32_t max_live = 0;  // slots of the largest schedule in the class
@@ -47,8 +47,6 @@ struct SweepClass {
   uint32_t vals_bytes = 0, rec_buf = 0;
   size_t smem = 0;
   int threads = 0, blocks = 0;
-  const uint32_t* dd_circ_ids = nullptr;
-  const unsigned long long* dd_item_prefix = nullptr;
 };
 
 // Device bytes a job needs beyond its static arrays: good values, sweep
@@ -63,7 +61,7 @@ class BatchExec {
   size_t smem_optin = 0, smem_per_sm = 0;
 
   DevBuf d_static, d_desc, d_work, d_res;
-  DevBuf d_ctl;  // [0]: error flag; [1 + class index]: the class's work counter
+  DevBuf d_ctl;  // [0]: error flag; then one work counter per swept circuit
   PinnedBuf h_static, h_desc, h_res;
 
   std::vector<BatchCirc> circs;
@@ -79,7 +77,8 @@ class BatchExec {
   uint32_t n_circ = 0;
   bool tile0 = false;
   uint64_t static_bytes = 0, desc_bytes = 0;
-  uint64_t ctl_bytes = 256;  // error flag + one work counter per class
+  uint64_t ctl_bytes = 256;  // error flag + one work counter per swept circuit
+  BatchSweepParams params{};  // launch parameters being built (32 KB)
   size_t smem_attr[4] = {0, 0, 0, 0};  // dynamic smem limit set per words-per-item kernel
   cudaEvent_t* class_events = nullptr;  // direct launches: recorded after each class
   // Classes run as concurrent branches (one stream each), so CTAs of small
@@ -120,8 +119,6 @@ class BatchExec {
   // Sets each class's dynamic shared-memory limit on its kernel (a
   // per-kernel attribute other launch sequences may have changed).
   void apply_attributes();
-  // Forgets the limits set so far (after another user of the kernels set its own).
-  void reset_attributes();
   // Enqueues the launch sequence; returns the number of kernels.  With
   // with_events, ev[0] is recorded after the good machine, ev[1] after the sweeps.
   uint64_t enqueue(cudaStream_t s, bool good_only, bool with_events, cudaEvent_t* ev);

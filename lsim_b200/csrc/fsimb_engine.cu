@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -74,32 +75,50 @@ void fsimb_handle::use_schedule(int M) {
   sched_uploaded = false;
 }
 
-void fsimb_handle::default_shape(std::vector<uint32_t> widths, uint32_t widest, int& M, int& occ,
-                                 int& threads) {
-  M = 0;
-  occ = 1;
-  threads = 0;
+namespace fsimb {
+
+void default_sweep_shape(const Plan& plan, const std::function<const Schedule&(int)>& sched_at,
+                         const std::function<int(int, int, size_t)>& occupancy,
+                         std::vector<uint32_t> widths, uint32_t widest, size_t smem_optin,
+                         size_t smem_per_sm, int& M, int& occ, int& threads) {
+  const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
   const size_t share2 = sweep_smem_share(smem_optin, smem_per_sm, 2);
   for (int m : {8, 4}) {
     // plan.max_live (no bank constraints) bounds every schedule's slots from below
     if (sweep_vals_bytes(plan.max_live, m) + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
-    const Schedule& sc = cached_schedule(m);
+    const Schedule& sc = sched_at(m);
     if (sc.max_live > kMaxSlots) continue;
     const uint32_t vals = sweep_vals_bytes(sc.max_live, m);
     if (vals + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
     const size_t smem = vals + std::min<size_t>(widest, (share2 - vals) / 32) * 32;
-    CK(sweep_set_smem(m, smem));
     int t = (int)std::min<uint32_t>(pick_sweep_threads(widths, m), sweep_max_threads(m));
-    for (; t > 64; t -= 32) {
-      int got = 0;
-      CK(sweep_occupancy(m, t, smem, &got));
-      if (got >= 2) break;
-    }
+    while (t > 64 && occupancy(m, t, smem) < 2) t -= 32;
     M = m;
     occ = 2;
     threads = t;
     return;
   }
+  M = 8;
+  while (M > 1 && sweep_vals_bytes(plan.max_live, M) > share1) M /= 2;
+  while (M > 1 && (sched_at(M).max_live > kMaxSlots || sweep_vals_bytes(sched_at(M).max_live, M) > share1))
+    M /= 2;
+  occ = 1;
+  threads = (int)std::min<uint32_t>(pick_sweep_threads(widths, M), sweep_max_threads(M));
+}
+
+}  // namespace fsimb
+
+void fsimb_handle::default_shape(std::vector<uint32_t> widths, uint32_t widest, int& M, int& occ,
+                                 int& threads) {
+  default_sweep_shape(
+      plan, [&](int m) -> const Schedule& { return cached_schedule(m); },
+      [&](int m, int t, size_t smem) {
+        CK(sweep_set_smem(m, smem));
+        int got = 0;
+        CK(sweep_occupancy(m, t, smem, &got));
+        return got;
+      },
+      std::move(widths), widest, smem_optin, smem_per_sm, M, occ, threads);
 }
 
 void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& widths, uint32_t widest) {
@@ -136,14 +155,6 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
   // its time carries a few percent of noise).
   int dM = 0, docc = 1, dT = 0;
   default_shape(widths, widest, dM, docc, dT);
-  if (!dM) {
-    const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
-    dM = 8;
-    while (dM > 1 && sweep_vals_bytes(plan.max_live, dM) > share1) dM /= 2;
-    while (dM > 1 && sweep_vals_bytes(cached_schedule(dM).max_live, dM) > share1) dM /= 2;
-    std::vector<uint32_t> w(widths);
-    dT = (int)std::min<uint32_t>(pick_sweep_threads(w, dM), sweep_max_threads(dM));
-  }
   float default_ms = -1;
   struct Cand {
     int M, occ, T;
@@ -200,17 +211,23 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     sa.rec_buf = rec_buf;
     sa.err = d_err.as<int>();
     const int nb = (int)std::min<uint64_t>((uint64_t)n_sms * got, (uint64_t)sa.n_list * sa.subtiles);
-    CK(cudaMemsetAsync(d_queue.p, 0, sizeof(int), s));
-    CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
-    CK(cudaEventRecord(tune_ev[0], s));
-    CK(launch_sweep(M, T, nb, smem, sa, s));
-    CK(cudaEventRecord(tune_ev[1], s));
-    CK(cudaEventSynchronize(tune_ev[1]));
-    int kerr = 0;
-    CK(cudaMemcpy(&kerr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+    // an untimed run of the first candidate warms the GPU up; then the
+    // fastest of two timed runs counts
+    float ms = 1e30f;
+    for (int rep = (&cd == &cands[0]) ? -1 : 0; rep < 2; ++rep) {
+      CK(cudaMemsetAsync(d_queue.p, 0, sizeof(int), s));
+      CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
+      CK(cudaEventRecord(tune_ev[0], s));
+      CK(launch_sweep(M, T, nb, smem, sa, s));
+      CK(cudaEventRecord(tune_ev[1], s));
+      CK(cudaEventSynchronize(tune_ev[1]));
+      int kerr = 0;
+      CK(cudaMemcpy(&kerr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
+      float x = 0;
+      CK(cudaEventElapsedTime(&x, tune_ev[0], tune_ev[1]));
+      if (rep >= 0) ms = std::min(ms, x);
+    }
     if (default_ms < 0 && M == dM && occ == docc && T == dT) {
       default_ms = ms;
       best_ms = ms;

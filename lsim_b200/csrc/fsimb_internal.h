@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -146,6 +147,17 @@ struct PinnedBuf {
   }
 };
 
+// Default sweep shape of a circuit: two CTAs per SM at 8 or 4 words per
+// item when the value slots leave room for at least 64 staged records (the
+// CTA size then lowered until two fit), else the largest words per item
+// whose slots fit one CTA per SM, with the width heuristic's CTA size.
+// sched_at(M) returns the schedule at M; occupancy(M, threads, smem) the
+// sweep kernel's CTAs per SM.
+void default_sweep_shape(const Plan& plan, const std::function<const Schedule&(int)>& sched_at,
+                         const std::function<int(int, int, size_t)>& occupancy,
+                         std::vector<uint32_t> widths, uint32_t widest, size_t smem_optin,
+                         size_t smem_per_sm, int& M, int& occ, int& threads);
+
 // A fresh value for fsimb_handle::gen: every change of a handle's circuit,
 // faults or patterns gets a number no other state of any handle had.
 uint64_t next_generation();
@@ -280,7 +292,7 @@ struct fsimb_handle {
   const fsimb::Schedule& cached_schedule(int M);
   // Makes `sched` the schedule at M (re-uploaded before the next sweep).
   void use_schedule(int M);
-  // Default sweep shape; M = 0 / threads = 0 leave the choice to run().
+  // default_sweep_shape for this circuit and the plain sweep kernel.
   void default_shape(std::vector<uint32_t> widths, uint32_t widest, int& M, int& occ, int& threads);
   // Times candidate shapes on a strided sample of tile 0's sweeps and keeps
   // the fastest in tuned_M / tuned_T / tuned_occ.  Needs the plan and the

@@ -449,61 +449,44 @@ __global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(
   }
 }
 
-// Batch form: items of many circuits of one shape class, in circuit order;
-// each item names (circuit, tile, sweep, subtile).  A CTA's items come in
-// increasing order, so it keeps the current circuit's item range and
-// descriptor in shared memory and looks a circuit up only when it moves on.
+// Batch form: the circuits of one launch, each with its own work counter.
+// Every CTA walks the circuits in order and takes (tile, sweep, subtile)
+// items of each until its counter runs out, so items are consumed in
+// circuit order as from one queue.  The loop index is uniform and the
+// circuit fields come from the kernel parameters: the compiler keeps the
+// pointers in uniform registers, as for k_sweep.
 template <int M>
-__global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64)) k_sweep_batch(BatchSweepArgs a) {
+__global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64))
+    k_sweep_batch(const __grid_constant__ BatchSweepParams p) {
   extern __shared__ __align__(16) uint64_t vals[];
   __shared__ unsigned long long acc[M];
   __shared__ __align__(8) uint64_t bars[2];
-  __shared__ unsigned long long s_item, s_lo, s_hi;
-  __shared__ uint32_t s_cidx, s_new;
-  __shared__ __align__(16) BatchCirc s_c;
+  __shared__ uint32_t s_item;
   SweepCta k;
-  sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc);
-  if (threadIdx.x == 0) {
-    s_lo = 0;
-    s_hi = 0;
-  }
-  const uint32_t subtiles = kTileWords / M;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const unsigned long long it = atomicAdd(a.queue, 1ull);
-      s_item = it;
-      s_new = 0;
-      if (it < a.n_items && (it < s_lo || it >= s_hi)) {  // last prefix <= it
-        const uint32_t lo = find_prefix(a.item_prefix, a.n_circ, it);
-        s_lo = a.item_prefix[lo];
-        s_hi = lo + 1 < a.n_circ ? a.item_prefix[lo + 1] : a.n_items;
-        s_cidx = a.circ_ids[lo];
-        s_new = 1;
+  sweep_cta_init<M>(k, vals, p.vals_bytes, p.rec_buf, bars, acc);
+  constexpr uint32_t subtiles = kTileWords / M;
+  for (uint32_t ci = 0; ci < p.n_circ; ++ci) {
+    const SweepCirc& c = p.c[ci];
+    const uint32_t per_tile = c.n_sweeps * subtiles;
+    for (;;) {
+      if (threadIdx.x == 0) {
+        const unsigned long long it = atomicAdd(p.queue + ci, 1ull);
+        s_item = it < c.n_items ? (uint32_t)it : 0xFFFFFFFFu;
       }
-    }
-    __syncthreads();
-    const unsigned long long item = s_item;
-    if (item >= a.n_items) return;
-    if (s_new) {
-      constexpr int nw = sizeof(BatchCirc) / 8;
-      static_assert(sizeof(BatchCirc) % 8 == 0, "BatchCirc is copied as 8-byte words");
-      if (threadIdx.x < nw)
-        reinterpret_cast<unsigned long long*>(&s_c)[threadIdx.x] =
-            reinterpret_cast<const unsigned long long*>(a.circs + s_cidx)[threadIdx.x];
       __syncthreads();
-    }
-    // s_item / s_lo / s_c are rewritten only after sweep_item's barriers.
-    const unsigned long long local = item - s_lo;
-    const uint64_t per_tile = (uint64_t)s_c.n_sweeps * subtiles;
-    const uint32_t tile = (uint32_t)(local / per_tile);
-    const uint64_t rem = local % per_tile;
-    const uint32_t si = (uint32_t)(rem / subtiles);
-    const uint32_t w0 = (uint32_t)(rem % subtiles) * M;
-    const SweepView v{s_c.recs, s_c.level, s_c.level_off, s_c.li_off, s_c.li, s_c.fi_off, s_c.fi_idx,
-                      s_c.type, s_c.good + (uint64_t)tile * s_c.N * 32, s_c.max_gate_level};
-    if (!sweep_item<M>(k, v, s_c.inj[si], w0, s_c.out + ((uint64_t)tile * s_c.n_sweeps + si) * 32)) {
-      if (threadIdx.x == 0) atomicExch(a.err, 1);
-      return;
+      const uint32_t item = s_item;
+      __syncthreads();  // s_item is rewritten only after every thread read it
+      if (item == 0xFFFFFFFFu) break;
+      const uint32_t tile = item / per_tile;
+      const uint32_t rem = item - tile * per_tile;
+      const uint32_t si = rem / subtiles;
+      const uint32_t w0 = (rem % subtiles) * M;
+      const SweepView v{c.recs, c.level, c.level_off, c.li_off, c.li, c.fi_off, c.fi_idx, c.type,
+                        c.good + (uint64_t)tile * c.N * 32, c.max_gate_level};
+      if (!sweep_item<M>(k, v, c.inj[si], w0, c.out + ((uint64_t)tile * c.n_sweeps + si) * 32)) {
+        if (threadIdx.x == 0) atomicExch(p.err, 1);
+        return;
+      }
     }
   }
 }
@@ -796,10 +779,10 @@ cudaError_t sweep_batch_occupancy(int M, int threads, size_t smem, int* blocks_p
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepArgs& a,
+cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepParams& p,
                                cudaStream_t s) {
   switch (M) {
-#define X(m) case m: k_sweep_batch<m><<<blocks, threads, smem, s>>>(a); break;
+#define X(m) case m: k_sweep_batch<m><<<blocks, threads, smem, s>>>(p); break;
     FSIMB_SWEEP_BATCH_CASES(X)
 #undef X
     default: return cudaErrorInvalidValue;

@@ -125,17 +125,33 @@ struct BatchCirc {
   uint32_t max_gate_level, n_levels;
 };
 
-struct BatchSweepArgs {
-  const BatchCirc* circs;
-  const uint32_t* circ_ids;                  // circuits of this launch, in item order
-  const unsigned long long* item_prefix;     // [n_circ] first item of each; items of a
-                                             // circuit are (tile, sweep, subtile), tile-major
-  uint32_t n_circ;
-  unsigned long long n_items;
-  unsigned long long* queue;
-  uint32_t vals_bytes, rec_buf;
-  int* err;
+// What the batched sweep reads of one circuit.  A launch carries these in
+// its parameters, so the compiler sees them as warp-uniform values.
+struct SweepCirc {
+  const uint4* recs;
+  const uint32_t* level;
+  const uint32_t* level_off;
+  const uint32_t* li_off;
+  const uint32_t* li;
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const InjRec* inj;
+  const uint64_t* good;  // [tiles][N][32]
+  uint64_t* out;         // [tiles][n_sweeps][32]
+  uint32_t N, n_sweeps, max_gate_level;
+  uint32_t n_items;      // tiles * n_sweeps * (32 / M): (tile, sweep, subtile), tile-major
 };
+
+constexpr int kSweepCircsPerLaunch = 300;
+
+struct BatchSweepParams {
+  SweepCirc c[kSweepCircsPerLaunch];
+  unsigned long long* queue;  // [n_circ] work counters, zero before the launch
+  int* err;
+  uint32_t n_circ, vals_bytes, rec_buf;
+};
+static_assert(sizeof(BatchSweepParams) <= 32000, "kernel parameters are limited to 32,764 bytes");
 
 // A level of the batched good machine: segments (circuit, element range)
 // with one warp per (element, tile).
@@ -154,7 +170,7 @@ struct BatchUnits {
 
 void launch_good_batch(const BatchCirc* circs, const BatchGoodSeg* segs, uint32_t n_segs,
                        unsigned long long n_units, cudaStream_t s);
-cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepArgs& a,
+cudaError_t launch_sweep_batch(int M, int threads, int blocks, size_t smem, const BatchSweepParams& p,
                                cudaStream_t s);
 cudaError_t sweep_batch_set_smem(int M, size_t smem);
 cudaError_t sweep_batch_occupancy(int M, int threads, size_t smem, int* blocks_per_sm);

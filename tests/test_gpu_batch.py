@@ -102,6 +102,21 @@ def test_graph_replay_direct_launches_and_shapes_agree(mix):
         _same(s.results(), ref)
 
 
+def test_repeated_direct_runs_keep_launch_limits(mix):
+    """A second run that reuses the layout launches every class within its
+    kernel's shared-memory limit (the large member first, a small one last:
+    choosing shapes queries the kernels with the small member's size)."""
+    ws, refs = mix
+    sims = _members([ws[6], ws[5]])
+    with Batch(0) as b:
+        for s in sims:
+            b.add(s)
+        for graph in (False, False, True, False):
+            b.run(graph=graph, concurrent=False)
+            _same(sims[0].results(), refs[6])
+            _same(sims[1].results(), refs[5])
+
+
 def test_member_changes_are_picked_up(mix):
     ws, refs = mix
     sims = _members(ws[:4])
