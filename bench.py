@@ -464,6 +464,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
     ap.add_argument("--circuits", type=int, default=256, help="batch size for --workload c4")
+    ap.add_argument("--shape", default="",
+                    help="with --profile: sweep shape 'words_per_item,block_threads,ctas_per_sm' "
+                         "(the one the bench's tuner chose), else the default shape")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed run of the workload (for profiler captures)")
     args = ap.parse_args()
@@ -472,8 +475,12 @@ def main():
         w = gen.workload(args.workload)
         sim = Simulator(0)
         sim.read_text(w["ckt"], w["flst"], w["ptn"])
+        shape = {}
+        if args.shape:
+            M, T, occ = (int(x) for x in args.shape.split(","))
+            shape = dict(words_per_item=M, block_threads=T, ctas_per_sm=occ)
         for _ in range(max(1, args.steps)):
-            sim.run()
+            sim.run(**shape)
         st = sim.stats()
         print(json.dumps({"workload": args.workload, "faults": sim.info().num_faults,
                           "patterns": sim.info().num_patterns, "stats": st}))
