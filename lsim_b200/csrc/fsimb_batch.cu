@@ -79,34 +79,72 @@ uint64_t batch_job_work_bytes(const BatchJob& j, bool first_tile_only) {
   const uint64_t tiles = first_tile_only ? 1 : std::max<uint64_t>(1, (j.pats->W + kTileWords - 1) / kTileWords);
   const uint64_t N = j.plan->N;
   const uint64_t ns = j.plan->sweeps.size();
-  uint64_t b = align256(tiles * N * kTileWords * 8);              // good
-  b += align256(tiles * std::max<uint64_t>(ns, 1) * kTileWords * 8);  // out
-  if (!first_tile_only) b += align256(tiles * N * kTileWords * 8);  // sens
-  b += 17 * j.F + 256;                                            // count, first, lastflag
+  const uint64_t slots = j.plan->members.size() + j.plan->roots.size();
+  uint64_t b = 0;
+  if (!j.good_resident) b += align256(tiles * N * kTileWords * 8);        // good
+  b += align256(tiles * std::max<uint64_t>(ns, 1) * kTileWords * 8);      // out
+  if (!first_tile_only) b += align256(tiles * std::max<uint64_t>(slots, 1) * kTileWords * 8);  // sens
   return b;
 }
 
 uint64_t batch_job_static_bytes(const BatchJob& j) {
   const Netlist& nl = *j.nl;
   const Plan& p = *j.plan;
-  const Schedule& sc = *j.sched;
   uint64_t b = 0;
   auto t = [&](uint64_t bytes) { b += align256(bytes); };
-  t(nl.type.size());
-  t(nl.fi_off.size() * 4);
-  t(nl.fi_idx.size() * 4);
-  t(nl.level.size() * 4);
-  t(p.level_off.size() * 4);
-  t(sc.recs.size() * sizeof(SweepRec));
-  t(sc.li_off.size() * 4);
-  t(sc.li.size() * 4);
+  if (!j.resident) {
+    const Schedule& sc = *j.sched;
+    t(nl.type.size());
+    t(nl.fi_off.size() * 4);
+    t(nl.fi_idx.size() * 4);
+    t(nl.level.size() * 4);
+    t(p.level_off.size() * 4);
+    t(sc.recs.size() * sizeof(SweepRec));
+    t(sc.li_off.size() * 4);
+    t(sc.li.size() * 4);
+  }
   t(p.sweeps.size() * sizeof(InjRec));
   t(p.roots.size() * sizeof(RootRec));
   t(p.members.size() * sizeof(MemberRec));
   t(p.traced.size() * sizeof(TracedRec));
+  t(p.traced_slot.size() * 4);
   t(p.exact_fault.size() * 4);
-  t(j.pats->words.size() * 8);
+  if (!j.good_resident) t(j.pats->words.size() * 8);
   return b;
+}
+
+uint32_t batch_job_good_segments(const BatchJob& j) {
+  if (j.good_resident) return 0;
+  uint32_t n = 0;
+  for (uint32_t l = 0; l < j.nl->n_levels; ++l) n += j.nl->level_off[l + 1] > j.nl->level_off[l];
+  return n;
+}
+
+WaveBytes batch_wave_bytes(const std::vector<BatchJob>& jobs, bool first_tile_only) {
+  WaveBytes w;
+  uint64_t F = 0, segs = 0, swept = 0;
+  for (const BatchJob& j : jobs) {
+    w.stat += batch_job_static_bytes(j);
+    w.work += batch_job_work_bytes(j, first_tile_only);
+    F += j.F;
+    segs += batch_job_good_segments(j);
+    swept += j.plan->sweeps.empty() ? 0 : 1;
+  }
+  const uint64_t n = jobs.size();
+  w.res = std::max<uint64_t>(F, 1) * 17 + 512;
+  w.desc = align256(n * sizeof(BatchCirc)) + align256(segs * sizeof(BatchGoodSeg)) + 2 * align256((n + 1) * 8);
+  w.ctl = align256((swept + 1) * 8);
+  return w;
+}
+
+WaveBytes batch_job_bytes(const BatchJob& j, bool first_tile_only) {
+  WaveBytes w;
+  w.stat = batch_job_static_bytes(j);
+  w.work = batch_job_work_bytes(j, first_tile_only);
+  w.res = 17 * j.F;
+  w.desc = sizeof(BatchCirc) + batch_job_good_segments(j) * sizeof(BatchGoodSeg) + 16;
+  w.ctl = 8;
+  return w;
 }
 
 void BatchExec::release() {
@@ -142,22 +180,34 @@ uint64_t BatchExec::upload_static(const std::vector<BatchJob>& jobs, cudaStream_
     const BatchJob& j = jobs[i];
     const Netlist& nl = *j.nl;
     const Plan& p = *j.plan;
-    const Schedule& sc = *j.sched;
     BatchCirc& c = circs[i];
-    c.type = (const uint8_t*)put(nl.type.data(), nl.type.size());
-    c.fi_off = (const uint32_t*)put(nl.fi_off.data(), nl.fi_off.size() * 4);
-    c.fi_idx = (const uint32_t*)put(nl.fi_idx.data(), nl.fi_idx.size() * 4);
-    c.level = (const uint32_t*)put(nl.level.data(), nl.level.size() * 4);
-    c.level_off = (const uint32_t*)put(p.level_off.data(), p.level_off.size() * 4);
-    c.recs = (const uint4*)put(sc.recs.data(), sc.recs.size() * sizeof(SweepRec));
-    c.li_off = (const uint32_t*)put(sc.li_off.data(), sc.li_off.size() * 4);
-    c.li = (const uint32_t*)put(sc.li.data(), sc.li.size() * 4);
+    if (j.resident) {  // circuit arrays already on the device
+      c.type = j.dev.type;
+      c.fi_off = j.dev.fi_off;
+      c.fi_idx = j.dev.fi_idx;
+      c.level = j.dev.level;
+      c.level_off = j.dev.level_off;
+      c.recs = j.dev.recs;
+      c.li_off = j.dev.li_off;
+      c.li = j.dev.li;
+    } else {
+      const Schedule& sc = *j.sched;
+      c.type = (const uint8_t*)put(nl.type.data(), nl.type.size());
+      c.fi_off = (const uint32_t*)put(nl.fi_off.data(), nl.fi_off.size() * 4);
+      c.fi_idx = (const uint32_t*)put(nl.fi_idx.data(), nl.fi_idx.size() * 4);
+      c.level = (const uint32_t*)put(nl.level.data(), nl.level.size() * 4);
+      c.level_off = (const uint32_t*)put(p.level_off.data(), p.level_off.size() * 4);
+      c.recs = (const uint4*)put(sc.recs.data(), sc.recs.size() * sizeof(SweepRec));
+      c.li_off = (const uint32_t*)put(sc.li_off.data(), sc.li_off.size() * 4);
+      c.li = (const uint32_t*)put(sc.li.data(), sc.li.size() * 4);
+    }
     c.inj = (const InjRec*)put(p.sweeps.data(), p.sweeps.size() * sizeof(InjRec));
     c.roots = (const RootRec*)put(p.roots.data(), p.roots.size() * sizeof(RootRec));
     c.members = (const MemberRec*)put(p.members.data(), p.members.size() * sizeof(MemberRec));
     c.traced = (const TracedRec*)put(p.traced.data(), p.traced.size() * sizeof(TracedRec));
+    c.traced_slot = (const uint32_t*)put(p.traced_slot.data(), p.traced_slot.size() * 4);
     c.exact_fault = (const uint32_t*)put(p.exact_fault.data(), p.exact_fault.size() * 4);
-    c.pwords = (const uint64_t*)put(j.pats->words.data(), j.pats->words.size() * 8);
+    c.pwords = j.good_resident ? nullptr : (const uint64_t*)put(j.pats->words.data(), j.pats->words.size() * 8);
   }
   if (at) CK(cudaMemcpyAsync(d_static.p, h_static.p, at, cudaMemcpyHostToDevice, s));
   static_bytes = at;
@@ -165,7 +215,7 @@ uint64_t BatchExec::upload_static(const std::vector<BatchJob>& jobs, cudaStream_
 }
 
 void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<ClassShape>& shapes,
-                       bool first_tile_only, bool with_static, cudaStream_t s) {
+                       bool first_tile_only, cudaStream_t s) {
   invalidate_graph();
   tile0 = first_tile_only;
   const size_t n = jobs.size();
@@ -177,23 +227,18 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
   sweep_alg_bytes = 0;
   good_gate_words = 0;
 
-  // Static per-circuit arrays: one block, 256-byte aligned arrays.
-  if (with_static) {
-    uint64_t sz = 0;
-    for (const BatchJob& j : jobs) sz += batch_job_static_bytes(j);
-    d_static.ensure(sz);
-    h_static.ensure(sz);
-    upload_static(jobs, s);
-  } else {
-    for (size_t i = 0; i < n; ++i) circs[i] = jobs[i].dev;
-  }
+  // Sizes of every block (the ones batch_wave_bytes reports: a caller that
+  // sized the buffers by it never sees them reallocated).
+  const WaveBytes wb_need = batch_wave_bytes(jobs, first_tile_only);
+  // Static arrays not resident on the device: one block, 256-byte aligned.
+  d_static.ensure(wb_need.stat);
+  h_static.ensure(wb_need.stat);
+  upload_static(jobs, s);
 
   // Work arena (good, sweep outputs, sensitivities) and per-fault results.
-  uint64_t wsz = 0;
-  for (const BatchJob& j : jobs) wsz += batch_job_work_bytes(j, first_tile_only) - 17 * j.F - 256;
-  d_work.ensure(wsz);
+  d_work.ensure(wb_need.work);
   for (const BatchJob& j : jobs) F_total += j.F;
-  d_res.ensure(std::max<uint64_t>(F_total, 1) * 17 + 512);
+  d_res.ensure(wb_need.res);
   {
     char* wb = d_work.as<char>();
     uint64_t at = 0;
@@ -221,9 +266,11 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
       c.n_exact = (uint32_t)p.exact_fault.size();
       c.max_gate_level = p.max_gate_level;
       c.n_levels = p.n_levels;
-      c.good = (uint64_t*)take((uint64_t)tiles * p.N * kTileWords * 8);
+      c.n_slots = (uint32_t)(p.members.size() + p.roots.size());
+      c.good = j.good_resident ? j.dev.good : (uint64_t*)take((uint64_t)tiles * p.N * kTileWords * 8);
       c.out = (uint64_t*)take((uint64_t)tiles * std::max<uint32_t>(c.n_sweeps, 1) * kTileWords * 8);
-      c.sens = first_tile_only ? nullptr : (uint64_t*)take((uint64_t)tiles * p.N * kTileWords * 8);
+      c.sens = first_tile_only ? nullptr
+                               : (uint64_t*)take((uint64_t)tiles * std::max<uint32_t>(c.n_slots, 1) * kTileWords * 8);
       res_off[i] = fo;
       fo += j.F;
       fault_patterns += j.F * j.pats->P;
@@ -256,7 +303,7 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
     unsigned long long u = 0;
     for (size_t i = 0; i < n; ++i) {
       const Netlist& nl = *jobs[i].nl;
-      if (l >= nl.n_levels) continue;
+      if (jobs[i].good_resident || l >= nl.n_levels) continue;
       const uint32_t lo = nl.level_off[l], hi = nl.level_off[l + 1];
       if (hi <= lo) continue;
       segs.push_back(BatchGoodSeg{(uint32_t)i, lo, hi, 0, u});
@@ -314,10 +361,8 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
   exact_units = exact_prefix[n];
 
   // Descriptor block: circuits, good segments, class tables, unit prefixes.
-  uint64_t dsz = align256(n * sizeof(BatchCirc)) + align256(segs.size() * sizeof(BatchGoodSeg)) +
-                 2 * align256((n + 1) * 8);
-  d_desc.ensure(dsz);
-  h_desc.ensure(dsz);
+  d_desc.ensure(wb_need.desc);
+  h_desc.ensure(wb_need.desc);
   {
     uint8_t* hb = h_desc.as<uint8_t>();
     char* db = d_desc.as<char>();
@@ -337,8 +382,8 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
   }
   // Control words: one work counter per class and the error flag.
   ctl_bytes = align256(((uint64_t)n_counters + 1) * 8);
-  d_ctl.ensure(ctl_bytes);
-  h_res.ensure(std::max<uint64_t>(F_total, 1) * 17 + 64);
+  d_ctl.ensure(wb_need.ctl);
+  h_res.ensure(wb_need.res);
   n_circ = (uint32_t)n;
   // Host staging must outlive the copies above.
   CK(cudaStreamSynchronize(s));
@@ -826,7 +871,7 @@ struct fsimb_batch {
     tx.smem_optin = smem_optin;
     tx.smem_per_sm = smem_per_sm;
     std::vector<BatchJob> js = jobs_for(sample, a);
-    tx.layout(js, a.shapes, true, true, s);
+    tx.layout(js, a.shapes, true, s);
     tx.enqueue(s, true, false, nullptr);  // good machine of the sampled tiles
     cudaEvent_t e0 = ev(0), e1 = ev(1);
     std::vector<ClassShape> cur = a.shapes;
@@ -944,7 +989,7 @@ void fsimb_batch::run(const fsimb_batch_opts* opts) {
   uint64_t h2d = 0;
   if (relayout) {
     laid = false;
-    exec.layout(jobs_for(all, a), a.shapes, false, true, s);
+    exec.layout(jobs_for(all, a), a.shapes, false, s);
     h2d = exec.static_bytes + exec.desc_bytes;
     laid_members = members;
     laid_gens = g;

@@ -32,7 +32,18 @@ struct BatchJob {
   uint64_t F = 0;
   int M = 4;
   int cls = 0;      // sweep class (index into the layout's shapes)
-  BatchCirc dev{};  // static device pointers, when the caller owns them
+  // resident: the circuit arrays (type, fi_off, fi_idx, level, level_off,
+  // recs, li_off, li) are dev's, already on the device.  good_resident:
+  // dev.good holds the job's good-machine tiles; no patterns are uploaded and
+  // no good machine runs for it.
+  bool resident = false;
+  bool good_resident = false;
+  BatchCirc dev{};
+};
+
+// Device bytes of a wave's blocks (what BatchExec::layout asks for).
+struct WaveBytes {
+  uint64_t stat = 0, work = 0, res = 0, desc = 0, ctl = 0;
 };
 
 struct SweepClass {
@@ -49,11 +60,16 @@ struct SweepClass {
   int threads = 0, blocks = 0;
 };
 
-// Device bytes a job needs beyond its static arrays: good values, sweep
-// outputs, sensitivities and per-fault results.
+// Device bytes of a job's work arena: good values (unless resident), sweep
+// outputs, sensitivities.
 uint64_t batch_job_work_bytes(const BatchJob& j, bool first_tile_only);
-// Device bytes of a job's static arrays (circuit, schedule, plan, patterns).
+// Device bytes of a job's uploaded arrays (circuit and schedule unless
+// resident, plan, patterns unless the good values are resident).
 uint64_t batch_job_static_bytes(const BatchJob& j);
+// The exact sizes layout() asks for, and one job's share of them (the wave's
+// sizes are at most the sum of its jobs' shares plus batch_wave_bytes({})).
+WaveBytes batch_wave_bytes(const std::vector<BatchJob>& jobs, bool first_tile_only);
+WaveBytes batch_job_bytes(const BatchJob& j, bool first_tile_only);
 
 class BatchExec {
  public:
@@ -103,11 +119,11 @@ class BatchExec {
   ~BatchExec() { release(); }
   void release();
   uint64_t device_bytes() const;
-  // Lays out the jobs (synchronises `s` before returning).  with_static:
-  // upload each job's static arrays; otherwise use jobs[i].dev.
-  // first_tile_only: only tile 0 of each job (the autotuner's sample).
+  // Lays out the jobs: uploads what is not resident, carves the work arena
+  // (synchronises `s` before returning).  first_tile_only: only tile 0 of
+  // each job (the autotuner's sample).
   void layout(const std::vector<BatchJob>& jobs, const std::vector<ClassShape>& shapes,
-              bool first_tile_only, bool with_static, cudaStream_t s);
+              bool first_tile_only, cudaStream_t s);
   // Packs the jobs' static arrays into the pinned staging block and copies it
   // to the device (the layout's pointers stay valid: same jobs, same sizes).
   // Returns the bytes copied.

@@ -642,26 +642,28 @@ __global__ void __launch_bounds__(256) k_ffr_batch(BatchUnits u, unsigned long l
   const uint32_t tile = (uint32_t)(local / c.n_roots);
   const uint32_t ri = (uint32_t)(local % c.n_roots);
   const TileView tv{c.type, c.fi_off, c.fi_idx, c.good + (uint64_t)tile * c.N * 32};
-  uint64_t* sens = c.sens + (uint64_t)tile * c.N * 32;
+  // compact sensitivities: slot i = members[i], slot n_members + r = root r
+  uint64_t* sens = c.sens + (uint64_t)tile * c.n_slots * 32;
   const uint64_t* obsv = c.out + (uint64_t)tile * c.n_sweeps * 32;
   const RootRec rr = c.roots[ri];
   const uint32_t w = tile * 32 + lane;
   const uint32_t bits = round_bits(c.P, c.W, w);
   uint64_t obs = rr.obs == kObsOne ? ~0ull : rr.obs == kObsZero ? 0ull : obsv[(uint64_t)rr.obs * 32 + lane];
   obs &= bits_mask(bits);
-  sens[(uint64_t)rr.root * 32 + lane] = ~0ull;
+  sens[(uint64_t)rr.slot * 32 + lane] = ~0ull;
   for (uint32_t i = rr.mem_begin; i < rr.mem_end; ++i) {
     const MemberRec m = c.members[i];
-    sens[(uint64_t)m.e * 32 + lane] = sens[(uint64_t)m.p * 32 + lane] & local_sens(tv, m.p, m.pin, lane);
+    sens[(uint64_t)i * 32 + lane] = sens[(uint64_t)m.p_slot * 32 + lane] & local_sens(tv, m.p, m.pin, lane);
   }
   for (uint32_t i = rr.flt_begin; i < rr.flt_end; ++i) {
     const TracedRec tr = c.traced[i];
+    const uint64_t st = sens[(uint64_t)c.traced_slot[i] * 32 + lane];
     uint64_t sv, gv;
     if (tr.pin == 0) {
-      sv = sens[(uint64_t)tr.elem * 32 + lane];
+      sv = st;
       gv = tv.good[(uint64_t)tr.elem * 32 + lane];
     } else {
-      sv = sens[(uint64_t)tr.elem * 32 + lane] & local_sens(tv, tr.elem, tr.pin - 1, lane);
+      sv = st & local_sens(tv, tr.elem, tr.pin - 1, lane);
       gv = tv.good[(uint64_t)c.fi_idx[c.fi_off[tr.elem] + tr.pin - 1] * 32 + lane];
     }
     const uint64_t D = sv & (gv ^ (tr.value ? ~0ull : 0ull)) & obs;

@@ -111,11 +111,12 @@ struct BatchCirc {
   const RootRec* roots;
   const MemberRec* members;
   const TracedRec* traced;
+  const uint32_t* traced_slot;
   const uint32_t* exact_fault;
   const uint64_t* pwords;        // [W][n_pi]
   uint64_t* good;                // [tiles][N][32]
   uint64_t* out;                 // [tiles][n_sweeps][32]
-  uint64_t* sens;                // [tiles][N][32]
+  uint64_t* sens;                // [tiles][n_slots][32]: members, then roots
   unsigned long long* count;     // per fault
   unsigned long long* first;
   uint8_t* lastflag;
@@ -123,6 +124,7 @@ struct BatchCirc {
   uint32_t N, n_pi, W, tiles;
   uint32_t n_sweeps, n_stem_sweeps, n_roots, n_exact;
   uint32_t max_gate_level, n_levels;
+  uint32_t n_slots, pad;         // sensitivity slots per tile
 };
 
 // What the batched sweep reads of one circuit.  A launch carries these in

@@ -27,8 +27,9 @@ uint32_t gate_family(uint8_t t) {
   }
 }
 
-void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
-  P = Plan();
+void build_circuit_plan(const Netlist& nl, CircuitPlan& C) {
+  C = CircuitPlan();
+  Plan& P = C.base;
   const uint32_t N = nl.N;
   P.N = N;
   P.n_pi = (uint32_t)nl.n_pi;
@@ -42,7 +43,7 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     P.max_level_width = std::max<uint32_t>(P.max_level_width, nl.level_off[l + 1] - nl.level_off[l]);
 
   // Per-element fanout facts.
-  std::vector<uint8_t> mux_below(N, 0);
+  C.mux_below.assign(N, 0);
   P.po_drv.assign(N, 0);
   P.gate_fo.assign(N, 0);
   P.maxfo_level.assign(N, 0);
@@ -62,9 +63,9 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     uint8_t hb = 0;
     for (uint32_t k = nl.fo_off[e]; k < nl.fo_off[e + 1]; ++k) {
       uint32_t c = nl.fo_idx[k];
-      hb |= (nl.type[c] == G_MUX) | mux_below[c];
+      hb |= (nl.type[c] == G_MUX) | C.mux_below[c];
     }
-    mux_below[e] = hb;
+    C.mux_below[e] = hb;
   }
 
   // Peak number of live values (interval graph of [level, highest consumer
@@ -83,77 +84,31 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     }
   }
 
-  // FFR roots.
-  std::vector<uint32_t> root(N);
+  // FFR roots: an element with exactly one consumer belongs to the FFR of that
+  // consumer; the members of each FFR, element-descending (consumer first).
+  C.root.resize(N);
   for (int64_t e = (int64_t)N - 1; e >= 0; --e) {
     uint32_t fo = nl.fo_off[e + 1] - nl.fo_off[e];
     if (nl.type[e] == G_PO || fo != 1)
-      root[e] = (uint32_t)e;
+      C.root[e] = (uint32_t)e;
     else
-      root[e] = root[nl.fo_idx[nl.fo_off[e]]];
+      C.root[e] = C.root[nl.fo_idx[nl.fo_off[e]]];
   }
-  auto reaches_po = [&](uint32_t x) {
-    return (nl.type[x] == G_PO || P.po_drv[x]) ? kInjReachesPo : 0u;
-  };
-  auto is_exact = [&](const Fault& ft) {
-    return ft.pin == 0 ? (bool)mux_below[ft.site] : (nl.type[ft.site] == G_MUX || mux_below[ft.site]);
-  };
-
-  // Classify faults.
-  std::vector<uint32_t> root_id(N, UINT32_MAX);
-  std::vector<std::vector<uint32_t>> root_faults;
-  std::vector<uint32_t> root_elem;
-  for (uint32_t f = 0; f < faults.size(); ++f) {
-    if (is_exact(faults[f])) continue;
-    uint32_t r = root[faults[f].site];
-    if (root_id[r] == UINT32_MAX) {
-      root_id[r] = (uint32_t)root_elem.size();
-      root_elem.push_back(r);
-      root_faults.emplace_back();
+  C.ffr_off.assign(N + 1, 0);
+  for (uint32_t e = 0; e < N; ++e)
+    if (C.root[e] != e) C.ffr_off[C.root[e] + 1]++;
+  for (uint32_t r = 0; r < N; ++r) C.ffr_off[r + 1] += C.ffr_off[r];
+  C.ffr_mem.resize(C.ffr_off[N]);
+  C.ffr_local.assign(N, 0);
+  {
+    std::vector<uint32_t> fill(C.ffr_off.begin(), C.ffr_off.end() - 1);
+    for (int64_t e = (int64_t)N - 1; e >= 0; --e) {
+      const uint32_t r = C.root[e];
+      if (r == (uint32_t)e) continue;
+      const uint32_t k = nl.fo_off[e];
+      C.ffr_local[e] = fill[r] - C.ffr_off[r];
+      C.ffr_mem[fill[r]++] = MemberRec{(uint32_t)e, nl.fo_idx[k], nl.fo_pin[k], 0};
     }
-    root_faults[root_id[r]].push_back(f);
-  }
-  // Members of the FFRs that carry traced faults, descending (consumer first).
-  std::vector<std::vector<uint32_t>> root_members(root_elem.size());
-  for (int64_t e = (int64_t)N - 1; e >= 0; --e) {
-    uint32_t r = root[e];
-    if (r != (uint32_t)e && root_id[r] != UINT32_MAX) root_members[root_id[r]].push_back((uint32_t)e);
-  }
-  // Order roots by topological index so neighbouring warps touch neighbouring data.
-  std::vector<uint32_t> rorder(root_elem.size());
-  for (uint32_t i = 0; i < rorder.size(); ++i) rorder[i] = i;
-  std::sort(rorder.begin(), rorder.end(), [&](uint32_t a, uint32_t b) { return root_elem[a] < root_elem[b]; });
-  for (uint32_t ri : rorder) {
-    const uint32_t r = root_elem[ri];
-    RootRec rr{};
-    rr.root = r;
-    if (nl.type[r] == G_PO || P.po_drv[r])
-      rr.obs = kObsOne;
-    else if (!P.gate_fo[r])
-      rr.obs = kObsZero;
-    else {
-      rr.obs = (uint32_t)P.sweeps.size();
-      P.sweeps.push_back(InjRec{r, 0, reaches_po(r), 0});
-      P.sweep_root.push_back((uint32_t)P.roots.size());
-    }
-    rr.mem_begin = (uint32_t)P.members.size();
-    for (uint32_t e : root_members[ri]) {
-      uint32_t k = nl.fo_off[e];
-      P.members.push_back(MemberRec{e, nl.fo_idx[k], nl.fo_pin[k], 0});
-    }
-    rr.mem_end = (uint32_t)P.members.size();
-    rr.flt_begin = (uint32_t)P.traced.size();
-    for (uint32_t f : root_faults[ri])
-      P.traced.push_back(TracedRec{f, faults[f].site, faults[f].pin, faults[f].value});
-    rr.flt_end = (uint32_t)P.traced.size();
-    P.roots.push_back(rr);
-  }
-  P.n_stem_sweeps = (uint32_t)P.sweeps.size();
-  for (uint32_t f = 0; f < faults.size(); ++f) {
-    const Fault& ft = faults[f];
-    if (!is_exact(ft)) continue;
-    P.sweeps.push_back(InjRec{ft.site, ft.pin, kInjStuck | reaches_po(ft.site), ft.value});
-    P.exact_fault.push_back(f);
   }
 
   // Algorithmic bytes of one gate-word evaluation: its fanin words read and
@@ -163,14 +118,108 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
     uint32_t nf = e < P.n_pi ? 0 : eff_fanin(nl, e);
     P.nfp_prefix[e + 1] = P.nfp_prefix[e] + 8ull * (nf + 1);
   }
+}
+
+void build_fault_plan(const Netlist& nl, const CircuitPlan& C, const std::vector<Fault>& faults,
+                      Plan& P) {
+  const Plan& B = C.base;
+  P = Plan();
+  P.N = B.N;
+  P.n_pi = B.n_pi;
+  P.n_gates = B.n_gates;
+  P.n_po = B.n_po;
+  P.n_levels = B.n_levels;
+  P.level_off = B.level_off;
+  P.max_gate_level = B.max_gate_level;
+  P.max_level_width = B.max_level_width;
+  P.max_live = B.max_live;
+  P.has_mux = B.has_mux;
+  auto reaches_po = [&](uint32_t x) {
+    return (nl.type[x] == G_PO || B.po_drv[x]) ? kInjReachesPo : 0u;
+  };
+  auto is_exact = [&](const Fault& ft) {
+    return ft.pin == 0 ? (bool)C.mux_below[ft.site]
+                       : (nl.type[ft.site] == G_MUX || C.mux_below[ft.site]);
+  };
+
+  // Traced faults grouped by FFR root (fault order within a root), roots in
+  // topological order so neighbouring warps touch neighbouring data.
+  std::vector<std::pair<uint32_t, uint32_t>> rf;  // (root, fault)
+  rf.reserve(faults.size());
+  for (uint32_t f = 0; f < faults.size(); ++f)
+    if (!is_exact(faults[f])) rf.emplace_back(C.root[faults[f].site], f);
+  std::stable_sort(rf.begin(), rf.end(),
+                   [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
+                     return a.first < b.first;
+                   });
+  for (size_t i = 0; i < rf.size();) {
+    const uint32_t r = rf[i].first;
+    RootRec rr{};
+    rr.root = r;
+    if (nl.type[r] == G_PO || B.po_drv[r])
+      rr.obs = kObsOne;
+    else if (!B.gate_fo[r])
+      rr.obs = kObsZero;
+    else {
+      rr.obs = (uint32_t)P.sweeps.size();
+      P.sweeps.push_back(InjRec{r, 0, reaches_po(r), 0});
+      P.sweep_root.push_back((uint32_t)P.roots.size());
+    }
+    rr.mem_begin = (uint32_t)P.members.size();
+    // a member's slot is its index in members; its consumer is the root
+    // (patched below, once the number of members is known) or a member of
+    // the same FFR listed before it
+    for (uint32_t k = C.ffr_off[r]; k < C.ffr_off[r + 1]; ++k) {
+      MemberRec m = C.ffr_mem[k];
+      m.p_slot = m.p == r ? kNoSlot : rr.mem_begin + C.ffr_local[m.p];
+      P.members.push_back(m);
+    }
+    rr.mem_end = (uint32_t)P.members.size();
+    rr.flt_begin = (uint32_t)P.traced.size();
+    for (; i < rf.size() && rf[i].first == r; ++i) {
+      const Fault& ft = faults[rf[i].second];
+      P.traced.push_back(TracedRec{rf[i].second, ft.site, ft.pin, ft.value});
+      P.traced_slot.push_back(ft.site == r ? kNoSlot : rr.mem_begin + C.ffr_local[ft.site]);
+    }
+    rr.flt_end = (uint32_t)P.traced.size();
+    P.roots.push_back(rr);
+  }
+  // root slots follow the members
+  const uint32_t n_mem = (uint32_t)P.members.size();
+  for (uint32_t ri = 0; ri < P.roots.size(); ++ri) {
+    RootRec& rr = P.roots[ri];
+    rr.slot = n_mem + ri;
+    for (uint32_t k = rr.mem_begin; k < rr.mem_end; ++k)
+      if (P.members[k].p_slot == kNoSlot) P.members[k].p_slot = rr.slot;
+    for (uint32_t k = rr.flt_begin; k < rr.flt_end; ++k)
+      if (P.traced_slot[k] == kNoSlot) P.traced_slot[k] = rr.slot;
+  }
+  P.n_stem_sweeps = (uint32_t)P.sweeps.size();
+  for (uint32_t f = 0; f < faults.size(); ++f) {
+    const Fault& ft = faults[f];
+    if (!is_exact(ft)) continue;
+    P.sweeps.push_back(InjRec{ft.site, ft.pin, kInjStuck | reaches_po(ft.site), ft.value});
+    P.exact_fault.push_back(f);
+  }
+
   const uint32_t gates_end = nl.level_off[std::min(P.max_gate_level + 1, nl.n_levels)];
   for (auto& s : P.sweeps) {
     uint32_t L0 = nl.level[s.elem] + 1;
     if (L0 <= P.max_gate_level) {
       P.dense_sweep_gates += gates_end - nl.level_off[L0];
-      P.dense_sweep_bytes += P.nfp_prefix[gates_end] - P.nfp_prefix[nl.level_off[L0]];
+      P.dense_sweep_bytes += B.nfp_prefix[gates_end] - B.nfp_prefix[nl.level_off[L0]];
     }
   }
+}
+
+void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
+  CircuitPlan C;
+  build_circuit_plan(nl, C);
+  build_fault_plan(nl, C, faults, P);
+  P.maxfo_level = std::move(C.base.maxfo_level);
+  P.gate_fo = std::move(C.base.gate_fo);
+  P.po_drv = std::move(C.base.po_drv);
+  P.nfp_prefix = std::move(C.base.nfp_prefix);
 }
 
 // ---------------------------------------------------------------- schedule

@@ -68,14 +68,15 @@ struct RootRec {
   uint32_t mem_end;
   uint32_t flt_begin;  // into traced faults
   uint32_t flt_end;
-  uint32_t pad[2];
+  uint32_t slot;       // compact sensitivity slot of the root: members.size() + root index
+  uint32_t pad;
 };
 
 struct MemberRec {  // internal FFR element e, its consumer p and pin position
   uint32_t e;
   uint32_t p;
   uint32_t pin;
-  uint32_t pad;
+  uint32_t p_slot;  // compact sensitivity slot of p (a member's slot is its index in members)
 };
 
 struct TracedRec {  // one traced fault
@@ -109,12 +110,27 @@ struct Plan {
   std::vector<RootRec> roots;
   std::vector<MemberRec> members;
   std::vector<TracedRec> traced;
+  std::vector<uint32_t> traced_slot;  // compact sensitivity slot of each traced fault's element
   // sweeps: first n_stem_sweeps are root flips, the rest exact faults
   std::vector<InjRec> sweeps;
   uint32_t n_stem_sweeps = 0;
   std::vector<uint32_t> exact_fault;  // fault index of each exact sweep
   std::vector<uint32_t> sweep_root;   // root record of each stem sweep
   bool has_mux = false;
+};
+
+// The fault-independent part of a plan, built once per circuit: `base` holds
+// the circuit fields of Plan (sizes, levels, fanout facts, live-value peak,
+// byte prefix sums; no roots or sweeps), plus what classifying a fault list
+// needs: MUX-below flags, the FFR root of every element and the members of
+// every FFR (element-descending, consumer first).
+struct CircuitPlan {
+  Plan base;
+  std::vector<uint8_t> mux_below;   // [N] some consumer path reaches a MUX
+  std::vector<uint32_t> root;       // [N] FFR root
+  std::vector<uint32_t> ffr_off;    // [N+1] members of the FFR rooted at r
+  std::vector<MemberRec> ffr_mem;
+  std::vector<uint32_t> ffr_local;  // [N] position of a member within its FFR's list
 };
 
 // Per-level evaluation order and shared-memory slots for one residue group
@@ -132,6 +148,13 @@ struct Schedule {
 // 0: AND family (AND, NAND, OR, NOR, INV, CLKBUF, PO), 1: XOR family, 2: MUX.
 uint32_t gate_family(uint8_t type);
 void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& plan);
+void build_circuit_plan(const Netlist& nl, CircuitPlan& cplan);
+// Roots, members, traced faults and sweeps of a fault list; the circuit's
+// per-element vectors (maxfo_level, gate_fo, po_drv, nfp_prefix) stay in
+// cplan.base and are left empty in `plan`.  Costs O(faults log faults +
+// members of the FFRs the faults touch).
+void build_fault_plan(const Netlist& nl, const CircuitPlan& cplan, const std::vector<Fault>& faults,
+                      Plan& plan);
 // G in {2, 4, 8, 16}.  A schedule that needs more than kMaxSlots slots
 // reports max_live > kMaxSlots and leaves li empty.
 void build_schedule(const Netlist& nl, const Plan& plan, uint32_t G, Schedule& out);
