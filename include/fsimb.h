@@ -33,6 +33,7 @@ extern "C" {
 #define FSIMB_ERR_NOMEM 5   /* host or device allocation failed */
 #define FSIMB_ERR_IO 6      /* file could not be opened or read */
 #define FSIMB_ERR_LIMIT 7   /* circuit exceeds a documented limit */
+#define FSIMB_ERR_TIMEOUT 8 /* fsimb_server_wait: the request is not done yet */
 
 typedef struct fsimb_handle fsimb_handle;
 
@@ -254,6 +255,76 @@ typedef struct {
 int fsimb_batch_class_stats(const fsimb_batch* b, uint32_t index, fsimb_batch_class* out);
 /* Member indices (order of fsimb_batch_add) of a class; n >= its n_circuits. */
 int fsimb_batch_class_members(const fsimb_batch* b, uint32_t index, uint32_t* out, uint64_t n);
+
+/* ------------------------------------------------------------------ serving
+ * A request loop over resident circuits.  No counterpart in the reference.
+ * A circuit added to a server stays on the device with its sweep schedule
+ * and, optionally, a resident block of patterns whose good-machine values
+ * are computed once; a request names a fault subset and a range of those
+ * patterns (or brings its own patterns).  Requests are submitted from any
+ * thread and return a ticket at once; planner threads plan them, and a
+ * dispatcher runs them in waves on `slots` concurrent slots, each with a
+ * fixed device arena of `slot_bytes` allocated when the server starts: a
+ * wave takes planned requests in ticket order while they fit its slot, so
+ * admission is by device footprint and serving allocates no device memory.
+ * While one slot's wave runs, requests that arrive meanwhile are planned and
+ * launched on the next free slot, and their work overlaps on the GPU.
+ * A request's results equal fsimb_run's for the same circuit, faults and
+ * patterns (count mode).  All fsimb_server_* calls are thread-safe. */
+typedef struct fsimb_server fsimb_server;
+
+typedef struct {
+  uint32_t struct_size;
+  uint32_t slots;             /* waves in flight at once: 0 -> 2, at most 8 */
+  uint64_t slot_bytes;        /* device bytes of each slot's arena: 0 -> 4 GiB */
+  uint32_t max_wave_requests; /* 0 -> 256 */
+  uint32_t planner_threads;   /* host threads planning requests: 0 -> auto */
+} fsimb_server_opts;
+
+typedef struct {
+  uint32_t struct_size;
+  uint32_t circuit;           /* id from fsimb_server_add_circuit */
+  const uint32_t* site;       /* faults by topological index (as fsimb_set_faults) */
+  const uint8_t* pin;         /* NULL: output faults */
+  const uint8_t* value;
+  uint64_t n_faults;
+  uint64_t n_patterns;        /* patterns of the request */
+  uint64_t row0;              /* first row (64 patterns each) of the circuit's resident
+                                 block, a multiple of 32; rows row0 .. row0 +
+                                 ceil(n_patterns / 64) are the request's patterns */
+  const uint64_t* words;      /* or the request's own words [ceil(P/64)][nPI]; then row0
+                                 is ignored and its good machine runs in its wave */
+} fsimb_request;
+
+typedef struct {
+  uint64_t completed, failed, waves, circuits;
+  double mean_wave_requests;
+  double fault_patterns;      /* sum over completed requests of faults x patterns */
+  double wall_ms;             /* first submit to last completion since the reset */
+  double ms_gpu_busy;         /* sum of wave durations on the GPU (overlapping waves both count) */
+  double latency_p50_ms, latency_p99_ms, latency_mean_ms, latency_max_ms;  /* submit -> done */
+  double queue_p50_ms, queue_p99_ms;      /* submit -> wave launch */
+  double wave_gpu_p50_ms, wave_gpu_p99_ms;
+  uint64_t resident_bytes;    /* device bytes of the resident circuits */
+  uint64_t slot_bytes;        /* device bytes of the slots' arenas */
+} fsimb_server_stats;
+
+int fsimb_server_create(int device, const fsimb_server_opts* opts, fsimb_server** out);
+/* Finishes the requests in flight, then frees everything. */
+int fsimb_server_destroy(fsimb_server* s);
+const char* fsimb_server_last_error(const fsimb_server* s);
+/* Circuit text (.ckt) and an optional resident pattern block [ceil(P/64)][nPI]. */
+int fsimb_server_add_circuit(fsimb_server* s, const char* ckt, size_t ckt_len, const uint64_t* words,
+                             uint64_t n_patterns, uint32_t* id);
+int fsimb_server_submit(fsimb_server* s, const fsimb_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a ticket.  FSIMB_OK: the results
+ * are in out[0..n) and the ticket is released; FSIMB_ERR_TIMEOUT: not done
+ * yet; any other status: the request failed (message in last_error) and the
+ * ticket is released. */
+int fsimb_server_wait(fsimb_server* s, uint64_t ticket, fsimb_fault_result* out, uint64_t n,
+                      int64_t timeout_ms);
+int fsimb_server_get_stats(fsimb_server* s, fsimb_server_stats* out);
+int fsimb_server_reset_stats(fsimb_server* s);
 
 /* Synthetic workloads (seeded; text in LSIM's formats).  Returned buffers
  * are released with fsimb_free_text. */

@@ -7,4 +7,5 @@ of ``libfsimb200.so`` (include/fsimb.h).
 """
 from .simulator import Simulator, FsimbError, RESULT_DTYPE  # noqa: F401
 from .batch import Batch  # noqa: F401
+from .serve import Server  # noqa: F401
 from . import gen  # noqa: F401

@@ -12,8 +12,9 @@ from . import build as _build
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-OK, ERR_ARG, ERR_PARSE, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_IO, ERR_LIMIT = range(8)
-_ERR_NAMES = {1: "ARG", 2: "PARSE", 3: "CUDA", 4: "STATE", 5: "NOMEM", 6: "IO", 7: "LIMIT"}
+OK, ERR_ARG, ERR_PARSE, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_IO, ERR_LIMIT, ERR_TIMEOUT = range(9)
+_ERR_NAMES = {1: "ARG", 2: "PARSE", 3: "CUDA", 4: "STATE", 5: "NOMEM", 6: "IO", 7: "LIMIT",
+              8: "TIMEOUT"}
 
 
 class FsimbError(RuntimeError):
@@ -109,6 +110,32 @@ class BatchClass(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("slots", ctypes.c_uint32),
+                ("slot_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_uint32),
+                ("planner_threads", ctypes.c_uint32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("circuit", ctypes.c_uint32),
+                ("site", ctypes.POINTER(ctypes.c_uint32)), ("pin", ctypes.POINTER(ctypes.c_uint8)),
+                ("value", ctypes.POINTER(ctypes.c_uint8)), ("n_faults", ctypes.c_uint64),
+                ("n_patterns", ctypes.c_uint64), ("row0", ctypes.c_uint64),
+                ("words", ctypes.POINTER(ctypes.c_uint64))]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_uint64) for n in ["completed", "failed", "waves", "circuits"]] +
+                [(n, ctypes.c_double) for n in
+                 ["mean_wave_requests", "fault_patterns", "wall_ms", "ms_gpu_busy",
+                  "latency_p50_ms", "latency_p99_ms", "latency_mean_ms", "latency_max_ms",
+                  "queue_p50_ms", "queue_p99_ms", "wave_gpu_p50_ms", "wave_gpu_p99_ms"]] +
+                [("resident_bytes", ctypes.c_uint64), ("slot_bytes", ctypes.c_uint64)])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 # Every symbol the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _U64 = ctypes.c_uint64
@@ -159,6 +186,14 @@ SIGNATURES = {
     "fsimb_batch_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
     "fsimb_batch_class_stats": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(BatchClass)]),
     "fsimb_batch_class_members": (ctypes.c_int, [_P, ctypes.c_uint32, _U32P, _U64]),
+    "fsimb_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
+    "fsimb_server_destroy": (ctypes.c_int, [_P]),
+    "fsimb_server_last_error": (_CP, [_P]),
+    "fsimb_server_add_circuit": (ctypes.c_int, [_P, _CP, _SZ, _U64P, _U64, _U32P]),
+    "fsimb_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(Request), _U64P]),
+    "fsimb_server_wait": (ctypes.c_int, [_P, _U64, ctypes.POINTER(FaultResult), _U64, ctypes.c_int64]),
+    "fsimb_server_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
+    "fsimb_server_reset_stats": (ctypes.c_int, [_P]),
 }
 
 _lib = None

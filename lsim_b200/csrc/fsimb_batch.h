@@ -148,6 +148,9 @@ class BatchExec {
   void invalidate_graph();
   // Copies the per-fault counters and the error flag to the host (synchronises s).
   void fetch(cudaStream_t s, int* kerr);
+  // The same copies, queued on s without waiting; read_err() once they ran.
+  void fetch_async(cudaStream_t s);
+  int read_err() const;
   void results(size_t i, const BatchJob& j, fsimb_fault_result* out) const;
   uint64_t items() const;
 };

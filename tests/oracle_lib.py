@@ -84,6 +84,19 @@ class Oracle:
             raise ValueError(err.value.decode())
         self.P, self.W = P, W
 
+    def set_faults(self, site, pin, value):
+        """Faults by topological index (as fsimb_set_faults)."""
+        f = np.zeros(len(site), dtype=FAULT_DTYPE)
+        f["site"], f["pin"], f["value"] = site, pin, np.asarray(value) != 0
+        self.faults = f
+
+    def set_patterns(self, words, P):
+        """Pattern words [ceil(P/64)][nPI] (as fsimb_set_patterns)."""
+        self.P, self.W = P, (P + 63) // 64
+        self.words = np.ascontiguousarray(np.asarray(words, dtype=np.uint64).ravel())
+        if len(self.words) == 0:
+            self.words = np.zeros(1, dtype=np.uint64)
+
     def __del__(self):
         if getattr(self, "_nl", None):
             oracle_lib().or_free(self._nl)
