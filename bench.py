@@ -24,6 +24,12 @@ every gate output, 1,024-16,384 patterns) run as one batch (fsimb_batch_*,
 CUDA graph, autotuned sweep shape) against the same 256 circuits run one
 after another through the plain per-circuit path, both with inputs resident
 (value) and with every input copied from host memory each step (e2e).
+
+--workload c5 times the serving configuration: 32 resident circuits
+(gen.serve_configs: 1,000-500,000 gates), requests of 1,000-100,000 faults
+and 64-8,192 patterns served by the server (fsimb_server_*) and by the plain
+path one job at a time, all at once and at Poisson arrival rates; it reports
+p50/p99 latency and fault-patterns/s for both.
 """
 import argparse
 import json
@@ -454,6 +460,153 @@ def run_batch(args):
     b.close()
 
 
+def run_serve(args):
+    """Serving configuration: requests against 32 resident circuits, served
+    by the server (waves on concurrent slots) and by the plain path one job
+    at a time, at a burst and at Poisson arrival rates."""
+    import threading
+    import torch
+    from lsim_b200 import Server, Simulator, gen
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(0)
+    cfgs = gen.serve_configs(args.circuits if args.circuits != 256 else 32, seed=0)
+    block_P = 16384
+    circs = []
+    t0 = time.perf_counter()
+    for c in cfgs:
+        ckt = gen.circuit(c["n_gates"], c["n_pi"], c["n_po"], c["n_levels"], p_fanin3=c["p_fanin3"],
+                          seed=c["seed"])
+        flst = gen.faults(ckt, c["faults"])
+        ptn = gen.patterns(c["n_pi"], block_P, seed=c["seed"])
+        h = Simulator(-1)
+        h.read_text(ckt, flst, ptn)
+        site, pin, val = h.faults()
+        circs.append(dict(ckt=ckt, words=h.patterns(), site=site, pin=pin, value=val,
+                          gates=c["n_gates"]))
+    gen_s = time.perf_counter() - t0
+    # the request stream: circuit, fault subset (1,000-100,000, log-uniform,
+    # at most the circuit's list), 64-8,192 patterns from a tile-aligned window
+    n_req = args.requests
+    reqs = []
+    for _ in range(n_req):
+        ci = int(rng.integers(len(circs)))
+        c = circs[ci]
+        F = len(c["site"])
+        k = min(F, int(round(np.exp(rng.uniform(np.log(1000), np.log(100000))))))
+        idx = np.sort(rng.choice(F, size=k, replace=False))
+        P = int(rng.integers(64, 8193))
+        W = (P + 63) // 64
+        row0 = 32 * int(rng.integers(0, (256 - W) // 32 + 1))
+        reqs.append(dict(circuit=ci, site=c["site"][idx].copy(), pin=c["pin"][idx].copy(),
+                         value=c["value"][idx].copy(), P=P, row0=row0))
+    FP = sum(len(r["site"]) * r["P"] for r in reqs)
+
+    srv = Server(0, slots=args.slots, slot_bytes=args.slot_gib << 30)
+    t0 = time.perf_counter()
+    ids = [srv.add_circuit(c["ckt"], c["words"], block_P) for c in circs]
+    add_s = time.perf_counter() - t0
+    plains = []
+    for c in circs:
+        p = Simulator(0)
+        p.load_circuit(c["ckt"])
+        plains.append(p)
+
+    def serve_at(rate):
+        """rate = requests/s (None: all at once); returns latency quantiles."""
+        srv.reset_stats()
+        arrivals = np.zeros(n_req) if rate is None else np.cumsum(rng.exponential(1.0 / rate, n_req))
+        tickets = [None] * n_req
+        start = time.perf_counter() + 0.05
+
+        def client():
+            for i, r in enumerate(reqs):
+                d = start + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(ids[r["circuit"]], r["site"], r["value"], pin=r["pin"],
+                                        n_patterns=r["P"], row0=r["row0"])
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+        return {"rate_req_s": rate, "p50_ms": st["latency_p50_ms"], "p99_ms": st["latency_p99_ms"],
+                "mean_ms": st["latency_mean_ms"], "value": st["fault_patterns"] / (st["wall_ms"] / 1e3),
+                "waves": st["waves"], "mean_wave_requests": st["mean_wave_requests"],
+                "wall_ms": st["wall_ms"], "gpu_wave_ms_sum": st["ms_gpu_busy"]}
+
+    def plain_at(rate):
+        arrivals = np.zeros(n_req) if rate is None else np.cumsum(rng.exponential(1.0 / rate, n_req))
+        lat = []
+        start = time.perf_counter() + 0.05
+        for i, r in enumerate(reqs):
+            d = start + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            p = plains[r["circuit"]]
+            c = circs[r["circuit"]]
+            W = (r["P"] + 63) // 64
+            p.set_faults(r["site"], r["pin"], r["value"])
+            p.set_patterns(c["words"][r["row0"]:r["row0"] + W], r["P"])
+            p.run()
+            p.results()
+            lat.append((time.perf_counter() - (start + arrivals[i])) * 1e3)
+        wall = time.perf_counter() - start
+        lat = np.array(lat)
+        return {"rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "value": FP / wall}
+
+    # warm-up: one pass of the stream through each path
+    serve_at(None)
+    plain_at(None)
+    clocks = ClockSampler(0)
+    clocks.start()
+    burst_srv = serve_at(None)
+    burst_plain = plain_at(None)
+    cap = n_req / (FP / burst_plain["value"])  # plain path capacity, requests/s
+    rows = []
+    for f in args.rates:
+        rows.append({"load": f, "server": serve_at(f * cap), "plain": plain_at(f * cap)})
+    clk = clocks.stop()
+    # results of the mix equal the plain path's, request by request
+    same = True
+    for i in range(0, n_req, max(1, n_req // 16)):
+        r = reqs[i]
+        t = srv.submit(ids[r["circuit"]], r["site"], r["value"], pin=r["pin"], n_patterns=r["P"],
+                       row0=r["row0"])
+        got = srv.wait(t)
+        p = plains[r["circuit"]]
+        W = (r["P"] + 63) // 64
+        p.set_faults(r["site"], r["pin"], r["value"])
+        p.set_patterns(circs[r["circuit"]]["words"][r["row0"]:r["row0"] + W], r["P"])
+        p.run()
+        same &= bool(np.array_equal(got, p.results()))
+    st = srv.stats()
+    gates = [c["gates"] for c in circs]
+    line = {
+        "metric": "served fault×pattern evals/s with p50/p99 latency (32 resident circuits)",
+        "value": burst_srv["value"], "unit": UNIT, "n_gpus": 1, "steps": n_req, "warmup": n_req,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "c5: %d resident circuits of %d-%d gates (median %d), %d-pattern "
+                               "resident blocks; %d requests of 1,000-100,000 faults and 64-8,192 "
+                               "patterns" % (len(circs), min(gates), max(gates),
+                                             int(np.median(gates)), block_P, n_req),
+                   "fault_patterns": FP, "slots": args.slots, "slot_gib": args.slot_gib,
+                   "generate_s": gen_s, "add_circuits_s": add_s,
+                   "resident_bytes": st["resident_bytes"], "slot_bytes": st["slot_bytes"],
+                   "rates": "fractions of the plain path's burst capacity (%.2f requests/s)" % cap},
+        "burst": {"server": burst_srv, "plain": burst_plain},
+        "poisson": rows,
+        "results_equal_plain": same,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    srv.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,7 +616,13 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
-    ap.add_argument("--circuits", type=int, default=256, help="batch size for --workload c4")
+    ap.add_argument("--circuits", type=int, default=256,
+                    help="circuits for --workload c4 (default 256) or c5 (default 32)")
+    ap.add_argument("--requests", type=int, default=200, help="requests for --workload c5")
+    ap.add_argument("--rates", type=float, nargs="*", default=[0.5, 1.0, 2.0, 4.0],
+                    help="--workload c5 Poisson rates, as fractions of the plain path's capacity")
+    ap.add_argument("--slots", type=int, default=2, help="server slots for --workload c5")
+    ap.add_argument("--slot-gib", type=int, default=8, help="server slot arena GiB for c5")
     ap.add_argument("--shape", default="",
                     help="with --profile: sweep shape 'words_per_item,block_threads,ctas_per_sm' "
                          "(the one the bench's tuner chose), else the default shape")
@@ -489,6 +648,8 @@ def main():
         run_reference(args)
     elif args.workload == "c4":
         run_batch(args)
+    elif args.workload == "c5":
+        run_serve(args)
     else:
         run_ours(args)
 

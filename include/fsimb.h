@@ -265,8 +265,10 @@ int fsimb_batch_class_members(const fsimb_batch* b, uint32_t index, uint32_t* ou
  * thread and return a ticket at once; planner threads plan them, and a
  * dispatcher runs them in waves on `slots` concurrent slots, each with a
  * fixed device arena of `slot_bytes` allocated when the server starts: a
- * wave takes planned requests in ticket order while they fit its slot, so
- * admission is by device footprint and serving allocates no device memory.
+ * wave takes planned requests in ticket order while they fit its slot and
+ * its predicted GPU time stays within `max_wave_ms`, so admission is by
+ * device footprint, small requests are not held up behind large ones, and
+ * serving allocates no device memory.
  * While one slot's wave runs, requests that arrive meanwhile are planned and
  * launched on the next free slot, and their work overlaps on the GPU.
  * A request's results equal fsimb_run's for the same circuit, faults and
@@ -279,6 +281,9 @@ typedef struct {
   uint64_t slot_bytes;        /* device bytes of each slot's arena: 0 -> 4 GiB */
   uint32_t max_wave_requests; /* 0 -> 256 */
   uint32_t planner_threads;   /* host threads planning requests: 0 -> auto */
+  uint32_t max_wave_ms;       /* a wave's predicted GPU time limit (a request that alone
+                                 exceeds it runs alone): 0 -> 200 */
+  uint32_t reserved;          /* 0 */
 } fsimb_server_opts;
 
 typedef struct {

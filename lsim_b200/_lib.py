@@ -113,7 +113,8 @@ class BatchClass(ctypes.Structure):
 class ServerOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("slots", ctypes.c_uint32),
                 ("slot_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_uint32),
-                ("planner_threads", ctypes.c_uint32)]
+                ("planner_threads", ctypes.c_uint32), ("max_wave_ms", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class Request(ctypes.Structure):

@@ -86,6 +86,7 @@ struct Request {
   Plan plan;
   BatchJob job;
   WaveBytes bytes;
+  double work = 0;  // gate-word evaluations of its sweeps (the wave-time predictor)
   std::vector<fsimb_fault_result> results;
   int status = FSIMB_OK;
   std::string error;
@@ -141,6 +142,9 @@ struct fsimb_server {
   bool stat_any = false;
   Clock::time_point stat_first_submit, stat_last_done;
   double stat_busy_ms = 0;
+  // Gate-word evaluations per ms of waves so far (exponential average); it
+  // turns a request's work into a predicted wave time.
+  double gwe_per_ms = 3e8;
 
   ~fsimb_server() { shutdown(); }
 
@@ -404,6 +408,8 @@ struct fsimb_server {
         if (j.good_resident)
           j.dev.good = c.d_good.as<uint64_t>() + (r->row0 / kTileWords) * (uint64_t)c.nl.N * kTileWords;
         r->bytes = batch_job_bytes(j, false);
+        r->work = (double)r->plan.dense_sweep_gates * kTileWords *
+                  (double)std::max<uint64_t>(1, (r->pats.W + kTileWords - 1) / kTileWords);
         WaveBytes need = overhead();
         add(need, r->bytes);
         if (!slots.empty() && !fits(need, slots[0]->cap))
@@ -484,6 +490,9 @@ struct fsimb_server {
     float gpu = 0;
     cudaEventElapsedTime(&gpu, s.e0, s.e1);
     stat_busy_ms += gpu;
+    double work = 0;
+    for (Request* r : s.wave) work += r->work;
+    if (gpu > 1.0f && work > 0) gwe_per_ms = 0.8 * gwe_per_ms + 0.2 * (work / gpu);
     for (size_t i = 0; i < s.wave.size(); ++i) {
       Request* r = s.wave[i];
       if (kerr) {
@@ -527,11 +536,26 @@ struct fsimb_server {
         if (s.busy || ready.empty()) continue;
         WaveBytes need = overhead();
         const uint32_t max_n = opts.max_wave_requests ? opts.max_wave_requests : 256;
-        for (auto it = ready.begin(); it != ready.end() && s.wave.size() < max_n;) {
+        // The oldest ready request leads the wave (a single admitted request
+        // always fits an empty slot).  Later ones join in ticket order while
+        // the wave fits the slot and its predicted time stays within
+        // max_wave_ms, so small requests are not held up behind a large one
+        // in the same wave; one that does not fit lets later, smaller ones
+        // try (at most 128 looked at).
+        const double max_ms = opts.max_wave_ms ? (double)opts.max_wave_ms : 200.0;
+        double wave_ms = 0;
+        size_t looked = 0;
+        for (auto it = ready.begin(); it != ready.end() && s.wave.size() < max_n && looked < 128;
+             ++looked) {
           WaveBytes next = need;
           add(next, it->second->bytes);
-          if (!fits(next, s.cap)) break;  // keep ticket order: later requests wait
+          const double ms = it->second->work / gwe_per_ms;
+          if (!fits(next, s.cap) || (!s.wave.empty() && wave_ms + ms > max_ms)) {
+            ++it;
+            continue;
+          }
           need = next;
+          wave_ms += ms;
           s.wave.push_back(it->second);
           it = ready.erase(it);
         }

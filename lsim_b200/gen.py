@@ -109,3 +109,22 @@ def batch_configs(n_circuits=256, seed=0, gates=(500, 50000), levels=(10, 120),
                         seed=seed * 100003 + i + 1, n_patterns=P, faults=faults,
                         type_mask=type_mask))
     return out
+
+
+def serve_configs(n_circuits=32, seed=0, gates=(1000, 500000), levels=(20, 150)):
+    """Resident circuits of the serving configuration (c5): gate counts
+    log-uniform in ``gates``, levels uniform in ``levels`` but at least one
+    level per 1,500 gates (the level width of the 200k-gate configuration is
+    1,333) and at most a quarter of the gates, PIs and POs a 32nd of the
+    gates (16-1,000); SA0/SA1 on every gate output and input pin, collapsed."""
+    import numpy as np
+    rng = np.random.default_rng(seed + 7919)
+    out = []
+    for i in range(n_circuits):
+        g = int(round(np.exp(rng.uniform(np.log(gates[0]), np.log(gates[1])))))
+        lv = max(int(rng.integers(levels[0], levels[1] + 1)), -(-g // 1500))
+        lv = max(2, min(lv, g // 4))
+        io = int(min(1000, max(16, g // 32)))
+        out.append(dict(n_gates=g, n_pi=io, n_po=io, n_levels=lv, p_fanin3=0.6,
+                        seed=seed * 100003 + 5000 + i, faults="collapsed"))
+    return out

@@ -21,9 +21,10 @@ def _arr(a, dtype):
 
 
 class Server:
-    def __init__(self, device=0, slots=0, slot_bytes=0, max_wave_requests=0, planner_threads=0):
+    def __init__(self, device=0, slots=0, slot_bytes=0, max_wave_requests=0, planner_threads=0,
+                 max_wave_ms=0):
         o = _lib.ServerOpts(ctypes.sizeof(_lib.ServerOpts), slots, slot_bytes, max_wave_requests,
-                            planner_threads)
+                            planner_threads, max_wave_ms, 0)
         s = ctypes.c_void_p()
         check(_lib.lib().fsimb_server_create(device, ctypes.byref(o), ctypes.byref(s)), None,
               "fsimb_server_last_error")
