@@ -626,6 +626,7 @@ def main():
     ap.add_argument("--shape", default="",
                     help="with --profile: sweep shape 'words_per_item,block_threads,ctas_per_sm' "
                          "(the one the bench's tuner chose), else the default shape")
+    ap.add_argument("--drop", action="store_true", help="with --profile: fault dropping")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed run of the workload (for profiler captures)")
     args = ap.parse_args()
@@ -638,11 +639,17 @@ def main():
         if args.shape:
             M, T, occ = (int(x) for x in args.shape.split(","))
             shape = dict(words_per_item=M, block_threads=T, ctas_per_sm=occ)
+        t0 = time.perf_counter()
         for _ in range(max(1, args.steps)):
-            sim.run(**shape)
+            sim.run(drop=args.drop, **shape)
+        wall = time.perf_counter() - t0
         st = sim.stats()
-        print(json.dumps({"workload": args.workload, "faults": sim.info().num_faults,
-                          "patterns": sim.info().num_patterns, "stats": st}))
+        res = sim.results()
+        info = sim.info()
+        print(json.dumps({"workload": args.workload, "faults": info.num_faults,
+                          "patterns": info.num_patterns, "elements": info.num_elements,
+                          "mode": "drop" if args.drop else "count", "wall_s": wall,
+                          "detected": int(res["detected"].sum()), "stats": st}))
         return
     if args.impl == "reference":
         run_reference(args)

@@ -143,8 +143,10 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     launch_good_level(g, s);
   }
   CK(cudaGetLastError());
-  // every stride-th sweep: about 6% of them, at least 2,048 when there are
-  const uint32_t stride = std::max<uint32_t>(1, std::min<uint32_t>(16, n_sweeps / 2048));
+  // every stride-th sweep: at most 1 in 16 and about 4,096 of them, so a
+  // candidate's run stays short on large circuits
+  const uint32_t stride =
+      std::max<uint32_t>(1, std::max<uint32_t>(std::min<uint32_t>(16, n_sweeps / 2048), n_sweeps / 4096));
   std::vector<uint32_t> list;
   for (uint32_t i = 0; i < n_sweeps; i += stride) list.push_back(i);
   upload(d_tune_list, list, s);
@@ -160,7 +162,7 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     int M, occ, T;
   };
   std::vector<Cand> cands{{dM, docc, dT}};
-  for (int M : {8, 4, 2})
+  for (int M : {8, 4, 2, 1})
     for (int occ : {1, 2, 3, 4})
       for (int T : {128, 256, 384, 512, 768, 1024})
         if (!(M == dM && occ == docc && T == dT)) cands.push_back({M, occ, T});

@@ -13,8 +13,8 @@ from the previous level; POs are driven by sink gates of the top levels.
       SA0/SA1 on every gate output and input pin collapsed by equivalence,
       65,536 uniform patterns;
   c3  2,000,000 gates, 5,000 PI / 5,000 PO, 400 levels, 10% of gates with a
-      fanout target of 8-64 (the rest 1-3), output + input-pin faults
-      collapsed, 16,384 patterns with half of the PIs at P(1) = 0.2.
+      fanout target of 8-64 (the rest 1-3), SA0/SA1 on every gate output
+      (4,000,000 faults), 16,384 patterns with half of the PIs at P(1) = 0.2.
 
 ``batch_configs`` draws the batched configuration (c4): circuits with gate
 counts log-uniform in 500-50,000, 10-120 levels, SA0/SA1 on every gate
@@ -41,7 +41,7 @@ WORKLOADS = {
     "c2s": dict(n_gates=50000, n_pi=1000, n_po=1000, n_levels=38, p_fanin3=0.6, seed=0,
                 n_patterns=2048, faults="collapsed"),
     "c3": dict(n_gates=2000000, n_pi=5000, n_po=5000, n_levels=400, p_fanin3=0.6, seed=0,
-               n_patterns=16384, faults="collapsed", hub_frac=0.1, biased_pi_frac=0.5,
+               n_patterns=16384, faults="outputs", hub_frac=0.1, biased_pi_frac=0.5,
                p_one_biased=0.2),
 }
 
