@@ -210,9 +210,8 @@ __device__ __forceinline__ void gate_body(uint64_t* vals, const uint4 q, uint32_
                                           const uint64_t* good_row, PoAcc<M>& pacc) {
   constexpr int C = (M >= 2) ? M / 2 : 1;
   constexpr int VC = (M >= 2) ? 2 : 1;
-  const uint32_t t = meta & kRecTypeMask;
-  const uint64_t ii = bmask((kIiMask >> t) & 1u);
-  const uint64_t io = bmask((kIoMask >> t) & 1u);
+  const uint64_t ii = (meta & kRecIi) ? ~0ull : 0ull;
+  const uint64_t io = (meta & kRecIo) ? ~0ull : 0ull;
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     const int h = (pl + c) % C;
@@ -278,18 +277,15 @@ template <int M>
 __device__ __forceinline__ void gate_dispatch(uint64_t* vals, const uint4 q, int pl,
                                               const uint64_t* good_row, PoAcc<M>& pacc) {
   const uint32_t meta = q.z >> 16;
-  const uint32_t t = meta & kRecTypeMask;
-  const uint32_t fam = ((kXfMask >> t) & 1u) | (t == G_MUX ? 2u : 0u);
-  const uint32_t code = fam * 4 + ((meta >> kRecNfShift) & 3u);  // family, fan-in - 1
-  switch (code) {
+  switch ((meta >> kRecClassShift) & 15u) {  // dense class index from the host (gate_class)
     case 0: gate_body<M, 0, 1>(vals, q, meta, pl, good_row, pacc); break;
     case 1: gate_body<M, 0, 2>(vals, q, meta, pl, good_row, pacc); break;
     case 2: gate_body<M, 0, 3>(vals, q, meta, pl, good_row, pacc); break;
     case 3: gate_body<M, 0, 4>(vals, q, meta, pl, good_row, pacc); break;
-    case 5: gate_body<M, 1, 2>(vals, q, meta, pl, good_row, pacc); break;
-    case 6: gate_body<M, 1, 3>(vals, q, meta, pl, good_row, pacc); break;
-    case 7: gate_body<M, 1, 4>(vals, q, meta, pl, good_row, pacc); break;
-    case 10: gate_body<M, 2, 3>(vals, q, meta, pl, good_row, pacc); break;
+    case 4: gate_body<M, 1, 2>(vals, q, meta, pl, good_row, pacc); break;
+    case 5: gate_body<M, 1, 3>(vals, q, meta, pl, good_row, pacc); break;
+    case 6: gate_body<M, 1, 4>(vals, q, meta, pl, good_row, pacc); break;
+    case 7: gate_body<M, 2, 3>(vals, q, meta, pl, good_row, pacc); break;
     default: gate_generic<M>(vals, q, meta, pl, good_row, pacc); break;
   }
 }

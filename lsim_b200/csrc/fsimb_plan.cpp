@@ -18,6 +18,14 @@ uint32_t eff_fanin(const Netlist& nl, uint32_t e) {
 
 }  // namespace
 
+uint32_t gate_class(uint8_t type, uint32_t nf) {
+  const uint32_t fam = gate_family(type);
+  if (fam == 0 && nf >= 1 && nf <= 4) return nf - 1;
+  if (fam == 1 && nf >= 2 && nf <= 4) return 4 + nf - 2;
+  if (fam == 2 && nf == 3) return 7;
+  return kClassGeneric;
+}
+
 uint32_t gate_family(uint8_t t) {
   switch (t) {
     case G_XOR:
@@ -332,8 +340,12 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       SweepRec r{};
       const uint32_t nf = nf_of(e);
       for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)slot[nl.fi_idx[nl.fi_off[e] + k]];
-      uint32_t meta = (uint32_t)nl.type[e] & kRecTypeMask;
+      const uint8_t t = nl.type[e];
+      uint32_t meta = (uint32_t)t & kRecTypeMask;
       meta |= ((nf ? nf - 1 : 0) & 3u) << kRecNfShift;
+      meta |= gate_class(t, nf) << kRecClassShift;
+      if (t == G_OR || t == G_NOR) meta |= kRecIi;
+      if (t == G_INV || t == G_OR || t == G_NAND || t == G_XNOR) meta |= kRecIo;
       if (P.po_drv[e]) meta |= kRecPo;
       if (P.gate_fo[e]) {
         slot[e] = pool.alloc(o % G);

@@ -44,6 +44,12 @@ constexpr uint32_t kRecTypeMask = 15u;     // bits 0-3: gate type
 constexpr int kRecNfShift = 4;             // bits 4-5: fan-in - 1
 constexpr uint32_t kRecPo = 1u << 6;       // drives a PO
 constexpr uint32_t kRecHasSlot = 1u << 7;  // has gate consumers (value stored)
+constexpr int kRecClassShift = 8;          // bits 8-11: gate class (sweep code path)
+constexpr uint32_t kRecIi = 1u << 12;      // invert inputs (OR, NOR)
+constexpr uint32_t kRecIo = 1u << 13;      // invert output (INV, OR, NAND, XNOR)
+// Gate classes: 0-3 AND family with 1-4 inputs, 4-6 XOR family with 2-4
+// inputs, 7 MUX with 3 inputs, 8 any other combination (generic path).
+constexpr uint32_t kClassGeneric = 8;
 
 // InjRec::mode bit fields
 constexpr uint32_t kInjStuck = 1u;      // 0: flip the element's word, 1: stuck value
@@ -147,6 +153,7 @@ struct Schedule {
 
 // 0: AND family (AND, NAND, OR, NOR, INV, CLKBUF, PO), 1: XOR family, 2: MUX.
 uint32_t gate_family(uint8_t type);
+uint32_t gate_class(uint8_t type, uint32_t fanin);
 void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& plan);
 void build_circuit_plan(const Netlist& nl, CircuitPlan& cplan);
 // Roots, members, traced faults and sweeps of a fault list; the circuit's
