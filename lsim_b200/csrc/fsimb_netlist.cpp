@@ -49,12 +49,20 @@ struct Tok {
       fail(std::string("expected an unsigned integer for ") + field + ", got '" +
            std::string(p, std::min<size_t>(16, e - p)) + "'");
     }
+    // 19 digits always fit in 64 bits; only a 20th needs the overflow check
     uint64_t v = 0;
-    while (p < e && *p >= '0' && *p <= '9') {
-      uint64_t d = (uint64_t)(*p - '0');
+    int n = 0;
+    while (p < e && (unsigned)(*p - '0') < 10u && n < 19) {
+      v = v * 10 + (uint64_t)(*p - '0');
+      ++p;
+      ++n;
+    }
+    if (p < e && (unsigned)(*p - '0') < 10u) {
+      const uint64_t d = (uint64_t)(*p - '0');
       if (v > (UINT64_MAX - d) / 10) fail(std::string("integer overflow in ") + field);
       v = v * 10 + d;
       ++p;
+      if (p < e && (unsigned)(*p - '0') < 10u) fail(std::string("integer overflow in ") + field);
     }
     if (p < e && !is_ws(*p)) fail(std::string("malformed integer in ") + field);
     return v;
