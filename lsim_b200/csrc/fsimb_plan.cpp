@@ -2,6 +2,7 @@
 #include "fsimb_plan.h"
 
 #include <algorithm>
+#include <array>
 
 namespace fsimb {
 
@@ -272,12 +273,61 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
   // family (AND, NAND, OR, NOR, INV, CLKBUF) is io ^ AND(in ^ ii), the XOR
   // family io ^ XOR(in); MUX is its own family.
   auto cls_of = [&](uint32_t e) { return gate_family(nl.type[e]) * 8 + nf_of(e); };
-  auto res = [&](uint32_t e, uint32_t k) { return slot[nl.fi_idx[nl.fi_off[e] + k]] % G; };
+  // Record position k of element e reads its fanin perm[e][k]: the AND and
+  // XOR families are commutative, so the grouper may reorder their fanins
+  // (pin faults and FFR tracing use the netlist's pin order, not the
+  // records); MUX keeps its order.
+  std::vector<std::array<uint8_t, 4>> perm(N, std::array<uint8_t, 4>{0, 1, 2, 3});
+  auto res_in = [&](uint32_t e, uint32_t k) { return slot[nl.fi_idx[nl.fi_off[e] + k]] % G; };
+  // permutations of 2, 3 and 4 inputs
+  static const uint8_t kPerm2[2][4] = {{0, 1, 2, 3}, {1, 0, 2, 3}};
+  static const uint8_t kPerm3[6][4] = {{0, 1, 2, 3}, {0, 2, 1, 3}, {1, 0, 2, 3},
+                                       {1, 2, 0, 3}, {2, 0, 1, 3}, {2, 1, 0, 3}};
+  uint8_t perm4[24][4];
+  {
+    uint8_t a[4] = {0, 1, 2, 3};
+    int n = 0;
+    do {
+      for (int k = 0; k < 4; ++k) perm4[n][k] = a[k];
+      ++n;
+    } while (std::next_permutation(a, a + 4));
+  }
+  // Cost of element e in a group with residue masks used[]: repeated
+  // residues over its fanin positions, for the best order of its fanins
+  // (written to *best_p).
+  auto place_cost = [&](uint32_t e, const uint32_t (&used)[4], const uint8_t** best_p) {
+    const uint32_t nf = nf_of(e);
+    const bool comm = gate_family(nl.type[e]) != 2;
+    const uint8_t(*list)[4] = kPerm2;
+    int np = 1;
+    if (comm && nf == 2) {
+      list = kPerm2;
+      np = 2;
+    } else if (comm && nf == 3) {
+      list = kPerm3;
+      np = 6;
+    } else if (comm && nf == 4) {
+      list = perm4;
+      np = 24;
+    }
+    int best = 1 << 30;
+    for (int q = 0; q < np; ++q) {
+      int cost = 0;
+      for (uint32_t k = 0; k < nf; ++k) cost += (used[k] >> res_in(e, list[q][k])) & 1u;
+      if (cost < best) {
+        best = cost;
+        *best_p = list[q];
+        if (cost == 0) break;
+      }
+    }
+    return best;
+  };
   std::vector<uint32_t> order, leftover;
   // Groups of G consecutive positions inside one class.  Each member is the
-  // candidate adding the fewest repeated residues (per fanin position) to
-  // the group, none if possible; only the last, partial group of a class goes
-  // to a mixed tail at the end of the level.
+  // candidate (with its best fanin order) adding the fewest repeated
+  // residues per fanin position to the group, none if possible; only the
+  // last, partial group of a class goes to a mixed tail at the end of the
+  // level.
   auto make_groups = [&](std::vector<uint32_t>& pool_in, bool tail) {
     std::vector<uint8_t> taken(pool_in.size(), 0);
     size_t left = pool_in.size(), first_free = 0;
@@ -287,18 +337,18 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       while (n_grp < G && left > 0) {
         size_t best = SIZE_MAX;
         int best_cost = 1 << 30;
+        const uint8_t* best_perm = kPerm2[0];
         size_t scanned = 0;
         while (first_free < pool_in.size() && taken[first_free]) ++first_free;
         for (size_t c = first_free; c < pool_in.size() && scanned < 256; ++c) {
           if (taken[c]) continue;
           ++scanned;
-          const uint32_t e = pool_in[c];
-          const uint32_t nf = nf_of(e);
-          int cost = 0;
-          for (uint32_t k = 0; k < nf; ++k) cost += (used[k] >> res(e, k)) & 1u;
+          const uint8_t* pp = kPerm2[0];
+          const int cost = place_cost(pool_in[c], used, &pp);
           if (cost < best_cost) {
             best_cost = cost;
             best = c;
+            best_perm = pp;
             if (cost == 0) break;
           }
         }
@@ -306,7 +356,8 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
         const uint32_t e = pool_in[best];
         taken[best] = 1;
         --left;
-        for (uint32_t k = 0; k < nf_of(e); ++k) used[k] |= 1u << res(e, k);
+        for (uint32_t k = 0; k < 4; ++k) perm[e][k] = best_perm[k];
+        for (uint32_t k = 0; k < nf_of(e); ++k) used[k] |= 1u << res_in(e, perm[e][k]);
         order.push_back(e);
         ++n_grp;
       }
@@ -339,7 +390,7 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       const uint32_t e = order[o];
       SweepRec r{};
       const uint32_t nf = nf_of(e);
-      for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)slot[nl.fi_idx[nl.fi_off[e] + k]];
+      for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)slot[nl.fi_idx[nl.fi_off[e] + perm[e][k]]];
       const uint8_t t = nl.type[e];
       uint32_t meta = (uint32_t)t & kRecTypeMask;
       meta |= ((nf ? nf - 1 : 0) & 3u) << kRecNfShift;
