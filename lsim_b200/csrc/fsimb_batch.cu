@@ -26,6 +26,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <thread>
 #include <vector>
@@ -45,7 +46,8 @@ int m_slot(int M) { return M == 1 ? 0 : M == 2 ? 1 : M == 4 ? 2 : 3; }
 
 uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
 
-// Runs f(i) for i in [0, n) on up to hardware_concurrency threads.
+// Runs f(i) for i in [0, n) on up to hardware_concurrency threads; the
+// first exception a worker raised is rethrown on the calling thread.
 template <class F>
 void parallel_for(size_t n, F f) {
   const size_t nt = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
@@ -55,20 +57,19 @@ void parallel_for(size_t n, F f) {
   }
   std::vector<std::thread> ts;
   std::atomic<size_t> next{0};
-  std::vector<std::string> errs(nt);
+  std::vector<std::exception_ptr> errs(nt);
   for (size_t t = 0; t < nt; ++t)
     ts.emplace_back([&, t] {
       try {
         for (size_t i = next++; i < n; i = next++) f(i);
-      } catch (const LimitError& e) {
-        errs[t] = e.msg;
-      } catch (const std::exception& e) {
-        errs[t] = e.what();
+      } catch (...) {
+        errs[t] = std::current_exception();
+        next = n;  // the others stop at their next item
       }
     });
   for (auto& t : ts) t.join();
   for (auto& e : errs)
-    if (!e.empty()) throw LimitError{e};
+    if (e) std::rethrow_exception(e);
 }
 
 }  // namespace

@@ -188,3 +188,13 @@ def test_batch_configs_follow_the_batched_configuration():
     assert all(10 <= c["n_levels"] <= 120 for c in cfgs)
     assert all(1024 <= c["n_patterns"] <= 16384 for c in cfgs)
     assert cfgs == gen.batch_configs(256, seed=0)
+
+
+def test_serve_configs_follow_the_serving_configuration():
+    cfgs = gen.serve_configs(32, seed=0)
+    assert len(cfgs) == 32
+    g = np.array([c["n_gates"] for c in cfgs])
+    assert g.min() >= 1000 and g.max() <= 500000
+    # levels at most 1,500 gates wide, so every circuit's sweep fits shared memory
+    assert all(c["n_gates"] / c["n_levels"] <= 1500 for c in cfgs)
+    assert cfgs == gen.serve_configs(32, seed=0)
