@@ -87,6 +87,40 @@ def test_sweep_shapes_agree(M, threads):
     _assert_same(sim.results(), ref)
 
 
+@pytest.mark.parametrize("M,threads,occ", [(2, 256, 3), (4, 128, 2), (8, 64, 4), (1, 512, 2)])
+def test_ctas_per_sm_shapes_agree(M, threads, occ):
+    """Several CTAs per SM (smaller record buffers) give the same results."""
+    w = gen.generate(n_gates=1500, n_pi=24, n_po=16, n_levels=25, n_patterns=2500, seed=32,
+                     type_mask=gen.ALL_TYPES, faults="pins")
+    ref = Oracle(w["ckt"], w["flst"], w["ptn"]).simulate()
+    sim = _run(w, words_per_item=M, block_threads=threads, ctas_per_sm=occ)
+    _assert_same(sim.results(), ref)
+    assert sim.stats()["ctas_per_sm"] >= 1
+
+
+def test_autotuned_shape_agrees_and_is_kept():
+    """The first tuned run times candidate shapes, later runs reuse the
+    winner, and a new fault list is tuned again; results never change."""
+    w = gen.generate(n_gates=4000, n_pi=40, n_po=30, n_levels=40, n_patterns=5000, seed=33,
+                     type_mask=gen.ALL_TYPES, faults="collapsed")
+    ref = Oracle(w["ckt"], w["flst"], w["ptn"]).simulate()
+    sim = _run(w, tune=True)
+    assert sim.stats()["ms_tune"] > 0
+    _assert_same(sim.results(), ref)
+    sim.run(tune=True)
+    assert sim.stats()["ms_tune"] == 0
+    _assert_same(sim.results(), ref)
+    flst = gen.faults(w["ckt"], "outputs")
+    sim.set_fault_text(flst)
+    sim.run(tune=True)
+    assert sim.stats()["ms_tune"] > 0
+    _assert_same(sim.results(), Oracle(w["ckt"], flst, w["ptn"]).simulate())
+    sim.run(tune=True, drop=True)
+    r = sim.results()
+    ref2 = Oracle(w["ckt"], flst, w["ptn"]).simulate()
+    assert np.array_equal(r["first_pattern"], ref2["first"])
+
+
 def test_drop_mode_first_pattern():
     w = gen.generate(n_gates=2000, n_pi=32, n_po=32, n_levels=30, n_patterns=20000, seed=41,
                      faults="collapsed", biased_pi_frac=0.7, p_one_biased=0.05)
