@@ -630,6 +630,25 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="one untimed run of the workload (for profiler captures)")
     args = ap.parse_args()
+    if args.profile and args.workload == "c4":
+        # one batch of the batched configuration's first --circuits circuits,
+        # kernels launched directly (not through the graph)
+        from lsim_b200 import Batch, Simulator, gen
+        sims = []
+        for c in gen.batch_configs(args.circuits, seed=0):
+            w = gen.generate(**c)
+            s = Simulator(-1)
+            s.read_text(w["ckt"], w["flst"], w["ptn"])
+            sims.append(s)
+        b = Batch(0)
+        for s in sims:
+            b.add(s)
+        for _ in range(max(1, args.steps)):
+            b.run(graph=False)
+        print(json.dumps({"workload": "c4", "circuits": args.circuits, "stats": b.stats(),
+                          "classes": b.classes()}))
+        b.close()
+        return
     if args.profile:
         from lsim_b200 import Simulator, gen
         w = gen.workload(args.workload)
