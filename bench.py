@@ -14,7 +14,10 @@ e2e:   the same through the public API from host buffers: pattern words
        uploaded from pinned host memory and per-fault results read back every
        step.
 With N > 1 each rank simulates its own 65,536-pattern block (seed = rank)
-and the per-fault results are merged across ranks every step (weak scaling).
+and the per-fault results are merged across ranks every step (weak scaling);
+with --shard faults each rank simulates its part of the fault list (whole
+fanout-free-region groups, balanced by estimated cost) over the same
+patterns, merged the same way (strong scaling).
 --impl reference times LSIM's own CPU simulator (oracle/_ref, else the CPU
 port in oracle/) on a bounded sample of the same workload on all host cores.
 
@@ -226,9 +229,19 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     from lsim_b200 import Simulator, gen, shard
 
-    w = gen.workload(WORKLOAD, pattern_seed=rank)
+    faults_sharded = args.shard == "faults"
+    # pattern sharding: each rank its own 65,536-pattern block (weak scaling);
+    # fault sharding: one block, each rank its part of the fault list (strong)
+    w = gen.workload(WORKLOAD, pattern_seed=0 if faults_sharded else rank)
     sim = Simulator(local)
     sim.read_text(w["ckt"], w["flst"], w["ptn"])
+    F_all = sim.info().num_faults
+    my_faults = None
+    if faults_sharded and world > 1:
+        site, pin, val = sim.faults()
+        group, cost = sim.fault_costs()
+        my_faults = shard.split_faults(group, cost, world)[rank]
+        sim.set_faults(site[my_faults], pin[my_faults], val[my_faults])
     info = sim.info()
     F, P = info.num_faults, info.num_patterns
     words = sim.patterns()
@@ -239,6 +252,8 @@ def run_ours(args):
     def merge(res):
         if world == 1:
             return res
+        if faults_sharded:
+            return shard.merge_fault_shards(res, my_faults, F_all, info.num_rounds, device="cuda")
         return shard.merge_results(res, rank * P, rank == world - 1, world * info.num_rounds,
                                    device="cuda")
 
@@ -296,7 +311,7 @@ def run_ours(args):
         ms_e2e = float(t.item())
     del merged
 
-    units = float(world) * F * P * args.steps
+    units = (float(F_all) if faults_sharded else float(world) * F) * P * args.steps
     value = units / (ms / 1e3)
     e2e = units / (ms_e2e / 1e3)
     peak, peak_src = _peaks()
@@ -307,10 +322,12 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": _workload_desc(F), "faults": F, "patterns": P,
+        "scaling": "strong" if faults_sharded else "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic",
+        "config": {"workload": _workload_desc(F_all), "faults": F_all, "patterns": P,
                    "elements": info.num_elements, "mode": "count",
-                   "parallelism": "pattern-sharded x%d" % world if world > 1 else "1 GPU",
+                   "parallelism": ("1 GPU" if world == 1 else
+                                   "%s-sharded x%d" % ("fault" if faults_sharded else "pattern", world)),
                    "l2": "inputs larger than L2: good-machine words %.2f GB rewritten each step"
                          % (info.num_elements * info.num_rounds * 8 / 1e9),
                    "sweep": {"words_per_item": st["words_per_item"],
@@ -616,6 +633,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
+    ap.add_argument("--shard", default="patterns", choices=["patterns", "faults"],
+                    help="with --gpus N > 1: each rank its own pattern block (weak scaling, "
+                         "default) or its part of the fault list (strong scaling)")
     ap.add_argument("--circuits", type=int, default=256,
                     help="circuits for --workload c4 (default 256) or c5 (default 32)")
     ap.add_argument("--requests", type=int, default=200, help="requests for --workload c5")

@@ -155,6 +155,14 @@ int fsimb_gates_per_level(const fsimb_handle* h, uint64_t* out, uint64_t n);
 int fsimb_types(const fsimb_handle* h, uint8_t* out, uint64_t n);
 /* loaded faults: topological site, pin, value */
 int fsimb_faults(const fsimb_handle* h, uint32_t* site, uint8_t* pin, uint8_t* value, uint64_t n);
+/* How faults share work, for splitting a fault list across GPUs (no
+ * counterpart in the reference, which runs on one machine): group[f] names
+ * the sweep fault f needs -- faults with equal groups share one (the faults
+ * of one fanout-free region) -- and cost[f] estimates that group's work in
+ * gate evaluations per pattern word (the same value for every fault of the
+ * group).  Keep a group on one GPU and balance the groups' costs.  Works on
+ * host-only handles; either pointer may be NULL; n = num_faults. */
+int fsimb_fault_costs(fsimb_handle* h, uint64_t* group, uint64_t* cost, uint64_t n);
 /* loaded pattern words, n = rounds * nPI */
 int fsimb_patterns(const fsimb_handle* h, uint64_t* out, uint64_t n);
 /* Graphviz DOT text of the loaded circuit in the layout of the reference's

@@ -167,6 +167,7 @@ SIGNATURES = {
     "fsimb_types": (ctypes.c_int, [_P, _U8P, _U64]),
     "fsimb_faults": (ctypes.c_int, [_P, _U32P, _U8P, _U8P, _U64]),
     "fsimb_patterns": (ctypes.c_int, [_P, _U64P, _U64]),
+    "fsimb_fault_costs": (ctypes.c_int, [_P, _U64P, _U64P, _U64]),
     "fsimb_gen_circuit": (ctypes.c_int, [ctypes.POINTER(GenConfig), ctypes.POINTER(ctypes.c_void_p),
                                          ctypes.POINTER(_SZ)]),
     "fsimb_gen_faults": (ctypes.c_int, [_CP, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),

@@ -880,6 +880,42 @@ int fsimb_faults(const fsimb_handle* hc, uint32_t* site, uint8_t* pin, uint8_t* 
   API_END(h)
 }
 
+int fsimb_fault_costs(fsimb_handle* h, uint64_t* group, uint64_t* cost, uint64_t n) {
+  API_BEGIN(h)
+  if (!h->has_ckt || !h->has_faults) throw StateError{"load a circuit and faults first"};
+  if (n != h->faults.size()) throw ArgError{"buffer size must equal the fault count"};
+  if (!h->plan_valid) {
+    build_plan(h->nl, h->faults, h->plan);
+    h->plan_valid = true;
+    h->plan_uploaded = false;
+    h->sched_M = 0;
+    h->sched_uploaded = false;
+  }
+  const Plan& P = h->plan;
+  const Netlist& nl = h->nl;
+  const uint32_t gates_end = nl.level_off[std::min(P.max_gate_level + 1, nl.n_levels)];
+  auto sweep_gates = [&](uint32_t elem) -> uint64_t {
+    const uint32_t L0 = nl.level[elem] + 1;
+    return L0 <= P.max_gate_level ? gates_end - nl.level_off[L0] : 0;
+  };
+  // traced faults: one group per FFR root (its sweep, when it has one, plus
+  // the tracing of its members); exact faults: one group each
+  for (const RootRec& rr : P.roots) {
+    const uint64_t c = 1 + (rr.obs < kObsZero ? sweep_gates(rr.root) : 0) + (rr.mem_end - rr.mem_begin);
+    for (uint32_t i = rr.flt_begin; i < rr.flt_end; ++i) {
+      const uint32_t f = P.traced[i].fault;
+      if (group) group[f] = rr.root;
+      if (cost) cost[f] = c;
+    }
+  }
+  for (uint32_t j = 0; j < P.exact_fault.size(); ++j) {
+    const uint32_t f = P.exact_fault[j];
+    if (group) group[f] = (uint64_t)nl.N + j;
+    if (cost) cost[f] = 1 + sweep_gates(P.sweeps[P.n_stem_sweeps + j].elem);
+  }
+  API_END(h)
+}
+
 int fsimb_patterns(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
   fsimb_handle* h = const_cast<fsimb_handle*>(hc);
   API_BEGIN(h)

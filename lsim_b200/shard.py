@@ -1,11 +1,20 @@
-"""Pattern sharding across ranks (one process per GPU).
+"""Sharding across ranks (one process per GPU).
 
-Faults are independent given the good machine, and so are pattern rounds:
-rank r simulates every fault over its own contiguous block of rounds, and
-the per-fault results combine with one reduction -- count by SUM, first
-detecting pattern by MIN (after shifting by the block's first pattern),
-detected by OR -- while the reference-compatible last-round flag comes from
-the rank that holds the last round.  No data moves during simulation.
+Faults are independent given the good machine, and so are pattern rounds.
+
+Pattern sharding (weak scaling): rank r simulates every fault over its own
+contiguous block of rounds, and the per-fault results combine with one
+reduction -- count by SUM, first detecting pattern by MIN (after shifting by
+the block's first pattern), detected by OR -- while the reference-compatible
+last-round flag comes from the rank that holds the last round.
+
+Fault sharding (strong scaling): rank r simulates its own part of the fault
+list over all patterns.  The parts keep every group of faults that share a
+sweep (one fanout-free region, fsimb_fault_costs) together and balance the
+groups' estimated costs; results combine with the same reductions, each
+fault being present on exactly one rank.
+
+No data moves during simulation in either form.
 """
 import numpy as np
 
@@ -58,3 +67,77 @@ def merge_results(res, first_pattern, holds_last_round, total_rounds, group=None
     out["ref_last_round_flag"] = flag.cpu().numpy().astype(np.uint8)
     out["ref_last_rd"] = max(0, total_rounds - 1)
     return out
+
+
+def split_faults(group, cost, world):
+    """Fault indices of each rank: whole groups (faults sharing a sweep),
+    largest estimated cost first, each to the rank with the least cost so
+    far.  group / cost: per fault, from Simulator.fault_costs()."""
+    group = np.asarray(group)
+    cost = np.asarray(cost, dtype=np.float64)
+    uniq, inv = np.unique(group, return_inverse=True)
+    gcost = np.zeros(len(uniq))
+    np.maximum.at(gcost, inv, cost)
+    order = np.argsort(-gcost, kind="stable")
+    load = np.zeros(world)
+    owner = np.empty(len(uniq), dtype=np.int64)
+    for gi in order:
+        r = int(np.argmin(load))
+        owner[gi] = r
+        load[r] += gcost[gi]
+    fault_owner = owner[inv]
+    return [np.nonzero(fault_owner == r)[0] for r in range(world)]
+
+
+def _fill(n_faults, idx, res):
+    cnt = np.zeros(n_faults, dtype=np.int64)
+    first = np.full(n_faults, INT64_MAX, dtype=np.int64)
+    flag = np.zeros(n_faults, dtype=np.int64)
+    fp = res["first_pattern"].astype(np.int64)
+    cnt[idx] = res["count"].astype(np.int64)
+    first[idx] = np.where(fp < 0, INT64_MAX, fp)
+    flag[idx] = res["ref_last_round_flag"].astype(np.int64)
+    return cnt, first, flag
+
+
+def _assemble(cnt, first, flag, last_rd, dtype):
+    out = np.zeros(len(cnt), dtype=dtype)
+    out["count"] = cnt.astype(np.uint64)
+    out["detected"] = (cnt > 0).astype(np.uint8)
+    out["first_pattern"] = np.where(first == INT64_MAX, -1, first)
+    out["ref_last_round_flag"] = flag.astype(np.uint8)
+    out["ref_last_rd"] = last_rd
+    return out
+
+
+def combine_fault_shards(parts, n_faults):
+    """Results of the whole fault list from (fault indices, results) of every
+    part, on one process."""
+    cnt = np.zeros(n_faults, dtype=np.int64)
+    first = np.full(n_faults, INT64_MAX, dtype=np.int64)
+    flag = np.zeros(n_faults, dtype=np.int64)
+    last_rd, dtype = 0, None
+    for idx, res in parts:
+        c, f, g = _fill(n_faults, idx, res)
+        cnt += c
+        first = np.minimum(first, f)
+        flag += g
+        if len(res):
+            last_rd = int(res["ref_last_rd"][0])
+        dtype = res.dtype
+    return _assemble(cnt, first, flag, last_rd, dtype)
+
+
+def merge_fault_shards(res, idx, n_faults, total_rounds, group=None, device="cpu"):
+    """All-reduce the results of this rank's faults (indices idx) into the
+    results of the whole fault list (identical on every rank)."""
+    import torch
+    import torch.distributed as dist
+
+    c, f, g = _fill(n_faults, idx, res)
+    cnt, first, flag = (torch.from_numpy(x).to(device) for x in (c, f, g))
+    dist.all_reduce(cnt, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(first, op=dist.ReduceOp.MIN, group=group)
+    dist.all_reduce(flag, op=dist.ReduceOp.SUM, group=group)
+    return _assemble(cnt.cpu().numpy(), first.cpu().numpy(), flag.cpu().numpy(),
+                     max(0, total_rounds - 1), res.dtype)

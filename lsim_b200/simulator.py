@@ -210,6 +210,15 @@ class Simulator:
             v.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n))
         return s, p, v
 
+    def fault_costs(self):
+        """(group, cost) per fault: faults with the same group share one sweep;
+        cost estimates the group's work (see fsimb_fault_costs)."""
+        n = self.info().num_faults
+        g = np.zeros(n, dtype=np.uint64)
+        c = np.zeros(n, dtype=np.uint64)
+        self._check(_lib.lib().fsimb_fault_costs(self._h, _u64p(g), _u64p(c), n))
+        return g, c
+
     def dot(self):
         """Graphviz text of the circuit (the reference's visualization_graph layout)."""
         ptr, n = ctypes.c_void_p(), ctypes.c_size_t()

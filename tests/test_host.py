@@ -198,3 +198,32 @@ def test_serve_configs_follow_the_serving_configuration():
     # levels at most 1,500 gates wide, so every circuit's sweep fits shared memory
     assert all(c["n_gates"] / c["n_levels"] <= 1500 for c in cfgs)
     assert cfgs == gen.serve_configs(32, seed=0)
+
+
+def test_fault_costs_group_faults_that_share_a_sweep():
+    from lsim_b200 import shard
+    w = gen.generate(n_gates=3000, n_pi=30, n_po=20, n_levels=30, n_patterns=64, seed=9,
+                     faults="pins")
+    sim = Simulator(-1)
+    sim.read_text(w["ckt"], w["flst"], w["ptn"])
+    site, pin, val = sim.faults()
+    group, cost = sim.fault_costs()
+    assert len(group) == len(site) and np.all(cost >= 1)
+    # faults on one element always share a group, and a group has one cost
+    for g in np.unique(group)[:200]:
+        assert len(set(cost[group == g])) == 1
+    by_site = {}
+    for s, g in zip(site, group):
+        assert by_site.setdefault(int(s), int(g)) == int(g)
+    parts = shard.split_faults(group, cost, 3)
+    allf = np.sort(np.concatenate(parts))
+    assert np.array_equal(allf, np.arange(len(site)))      # every fault exactly once
+    owners = {}
+    for r, idx in enumerate(parts):
+        for g in np.unique(group[idx]):
+            assert owners.setdefault(int(g), r) == r        # a group is never split
+    loads = []
+    for idx in parts:
+        _, first = np.unique(group[idx], return_index=True)
+        loads.append(float(cost[idx][first].sum()))
+    assert max(loads) <= 1.2 * min(loads) + cost.max()      # balanced

@@ -69,3 +69,59 @@ def test_pattern_shards_merge_to_full_block(P):
         assert np.array_equal(m["detected"], ref["detected"])
         assert np.array_equal(m["ref_last_round_flag"], ref["ref_flag"])
         assert np.array_equal(m["ref_last_rd"], ref["ref_rd"])
+
+
+def _fault_worker(rank, world, port, w, q):
+    import torch.distributed as dist
+    from lsim_b200 import Simulator
+    from tests.oracle_lib import Oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        h = Simulator(-1)
+        h.read_text(w["ckt"], w["flst"], w["ptn"])
+        site, pin, val = h.faults()
+        group, cost = h.fault_costs()
+        idx = shard.split_faults(group, cost, world)[rank]
+        o = Oracle(w["ckt"], "0\n", w["ptn"])
+        o.set_faults(site[idx], pin[idx], val[idx])
+        r = o.simulate(threads=2)
+        res = np.zeros(len(r), dtype=_DT)
+        res["count"] = r["count"]
+        res["first_pattern"] = r["first"]
+        res["ref_last_round_flag"] = r["ref_flag"]
+        res["ref_last_rd"] = r["ref_rd"]
+        merged = shard.merge_fault_shards(res, idx, len(site), h.info().num_rounds)
+        q.put((rank, merged.tobytes()))
+    finally:
+        dist.destroy_process_group()
+
+
+_DT = np.dtype([("detected", np.uint8), ("ref_last_round_flag", np.uint8), ("pad", np.uint8, 6),
+                ("first_pattern", np.int64), ("count", np.uint64), ("ref_last_rd", np.uint64)])
+
+
+def test_fault_shards_merge_to_full_list():
+    """Each of 2 ranks simulates its part of the fault list over all patterns;
+    the merge equals one simulation of the whole list."""
+    w = gen.generate(n_gates=400, n_pi=12, n_po=10, n_levels=14, n_patterns=64 * 9 + 5, seed=78,
+                     faults="pins", type_mask=gen.ALL_TYPES)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fault_worker, args=(r, 2, port, w, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    outs = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    from tests.oracle_lib import Oracle
+    ref = Oracle(w["ckt"], w["flst"], w["ptn"]).simulate()
+    for rank in range(2):
+        m = np.frombuffer(outs[rank], dtype=_DT)
+        assert np.array_equal(m["count"], ref["count"])
+        assert np.array_equal(m["first_pattern"], ref["first"])
+        assert np.array_equal(m["detected"], ref["detected"])
+        assert np.array_equal(m["ref_last_round_flag"], ref["ref_flag"])
+        assert np.array_equal(m["ref_last_rd"], ref["ref_rd"])
