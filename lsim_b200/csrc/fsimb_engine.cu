@@ -816,7 +816,7 @@ int fsimb_get_info(const fsimb_handle* hc, fsimb_info* out) {
   out->num_gates = h->nl.n_gates;
   out->num_wires = h->nl.n_wires;
   out->num_elements = h->nl.N;
-  out->num_levels = h->nl.n_levels;
+  out->num_levels = h->nl.ref_per_level.empty() ? h->nl.n_levels : h->nl.ref_per_level.size();
   out->num_faults = h->has_faults ? h->faults.size() : 0;
   out->num_patterns = h->has_pats ? h->pats.P : 0;
   out->num_rounds = h->has_pats ? h->pats.W : 0;
@@ -845,7 +845,8 @@ int fsimb_levels(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
   API_BEGIN(h)
   if (!h->has_ckt) throw StateError{"no circuit loaded"};
   if (n != h->nl.N || !out) throw ArgError{"buffer size must equal the element count"};
-  for (uint64_t i = 0; i < n; ++i) out[i] = h->nl.level[i];
+  const auto& level = h->nl.ref_level.empty() ? h->nl.level : h->nl.ref_level;
+  for (uint64_t i = 0; i < n; ++i) out[i] = level[i];
   API_END(h)
 }
 
@@ -853,8 +854,9 @@ int fsimb_gates_per_level(const fsimb_handle* hc, uint64_t* out, uint64_t n) {
   fsimb_handle* h = const_cast<fsimb_handle*>(hc);
   API_BEGIN(h)
   if (!h->has_ckt) throw StateError{"no circuit loaded"};
-  if (n != h->nl.n_levels || !out) throw ArgError{"buffer size must equal the level count"};
-  std::copy(h->nl.per_level.begin(), h->nl.per_level.end(), out);
+  const auto& per = h->nl.ref_per_level.empty() ? h->nl.per_level : h->nl.ref_per_level;
+  if (n != per.size() || !out) throw ArgError{"buffer size must equal the level count"};
+  std::copy(per.begin(), per.end(), out);
   API_END(h)
 }
 

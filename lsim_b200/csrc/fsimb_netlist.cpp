@@ -11,9 +11,10 @@
 //     reference then indexes past `order` (fsim/simulation.cpp:797-819);
 //   * a PO without a driver, or a MUX with fewer than three inputs
 //     (fsim/simulation.cpp:1054-1056, 1072-1076 read missing inputs);
-//   * duplicate writes to one pin slot that leave the topological order not
-//     level-sorted (legal in the reference, unsupported here: the GPU path
-//     relies on level-contiguous element ranges).
+// Pin-slot gaps and repeated pins, which the reference accepts, are kept
+// with the reference's meaning (fanin = slots 1..count); when they leave the
+// element order not level-sorted, the schedule levels differ from the
+// reference's levels (finalize_netlist) and the results do not.
 // A PI that directly drives a PO is accepted and the PO copies the PI; the
 // reference writes past its gate array in that case (fsim/simulation.cpp:856-861).
 #include "fsimb_netlist.h"
@@ -82,25 +83,44 @@ struct Tok {
 
 void finalize_netlist(Netlist& nl) {
   const uint32_t N = nl.N;
-  // Levels (fsim/simulation.cpp:882-916): PIs 0, gates 1 + max fanin, POs max+1.
-  nl.level.assign(N, 0);
-  uint32_t max_level = 0;
   const uint32_t g0 = (uint32_t)nl.n_pi, g1 = (uint32_t)(nl.n_pi + nl.n_gates);
-  for (uint32_t t = g0; t < g1; ++t) {
-    uint32_t lv = 0;
-    for (uint32_t k = nl.fi_off[t]; k < nl.fi_off[t + 1]; ++k)
-      lv = std::max(lv, nl.level[nl.fi_idx[k]] + 1);
-    nl.level[t] = lv;
-    max_level = std::max(max_level, lv);
-  }
-  for (uint32_t t = g1; t < N; ++t) nl.level[t] = max_level + 1;
-  nl.n_levels = max_level + 2;
-  nl.per_level.assign(nl.n_levels, 0);
-  for (uint32_t t = 0; t < N; ++t) nl.per_level[nl.level[t]]++;
-  for (uint32_t t = 1; t < N; ++t) {
-    if (nl.level[t] < nl.level[t - 1])
-      throw ParseError{"ckt: duplicate pin assignments leave the topological order not level-sorted "
-                       "(element " + std::to_string(t) + "); unsupported"};
+  // Levels (fsim/simulation.cpp:882-916): PIs 0, gates 1 + max fanin, POs
+  // max+1.  `running` also keeps each gate at or above the gate before it in
+  // element order: the schedule's level, equal to the reference's whenever
+  // the element order is level-sorted.
+  auto levelize = [&](bool running, std::vector<uint32_t>& level) {
+    level.assign(N, 0);
+    uint32_t max_level = 0;
+    for (uint32_t t = g0; t < g1; ++t) {
+      uint32_t lv = running && t > g0 ? level[t - 1] : 0;
+      for (uint32_t k = nl.fi_off[t]; k < nl.fi_off[t + 1]; ++k)
+        lv = std::max(lv, level[nl.fi_idx[k]] + 1);
+      level[t] = lv;
+      max_level = std::max(max_level, lv);
+    }
+    for (uint32_t t = g1; t < N; ++t) level[t] = max_level + 1;
+    return max_level + 2;
+  };
+  auto histogram = [&](const std::vector<uint32_t>& level, uint32_t n_levels) {
+    std::vector<uint64_t> h(n_levels, 0);
+    for (uint32_t t = 0; t < N; ++t) h[level[t]]++;
+    return h;
+  };
+  nl.n_levels = levelize(false, nl.level);
+  nl.per_level = histogram(nl.level, nl.n_levels);
+  nl.ref_level.clear();
+  nl.ref_per_level.clear();
+  bool sorted = true;
+  for (uint32_t t = 1; t < N && sorted; ++t) sorted = nl.level[t] >= nl.level[t - 1];
+  if (!sorted) {
+    // Pin-slot gaps or repeated pins drop an edge from a gate's fanin while
+    // the edge still orders the gate (fsim/simulation.cpp:697-703, 851-877):
+    // keep the reference's levels for the level queries and schedule by the
+    // running levels, which every fanin precedes.
+    nl.ref_level.swap(nl.level);
+    nl.ref_per_level.swap(nl.per_level);
+    nl.n_levels = levelize(true, nl.level);
+    nl.per_level = histogram(nl.level, nl.n_levels);
   }
   nl.level_off.assign(nl.n_levels + 1, 0);
   {

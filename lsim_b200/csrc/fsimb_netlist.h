@@ -9,7 +9,8 @@
 //   * fanin order    = pin-slot table, slots 1..count (fsim/simulation.cpp:684-711,
 //                      851-877), pin 5 (MUX select) remapped to slot 3;
 //   * levels         = PIs 0, gates 1+max(fanin), POs max+1
-//                      (fsim/simulation.cpp:882-916);
+//                      (fsim/simulation.cpp:882-916), raised to stay sorted
+//                      in element order where pin-slot gaps break that;
 //   * faults         = file id -> topological index, value 0 / ~0
 //                      (fsim/simulation.cpp:943-959);
 //   * patterns       = ceil(P/64) rows of nPI words (fsim/simulation.cpp:961-976).
@@ -53,6 +54,13 @@ struct Netlist {
   std::vector<uint64_t> tpg;      // [N] file id -> topological index
   std::vector<uint64_t> per_level;  // [n_levels] element count per level
   std::vector<uint32_t> level_off;  // [n_levels+1] first topological index of each level
+  // The reference's levels and per-level counts where they differ from
+  // `level` / `per_level` (element order not level-sorted by them); empty
+  // otherwise.  `level` is then the schedule level: 1 + max fanin level and
+  // at least the level of the element before, so level ranges stay
+  // contiguous in element order.
+  std::vector<uint32_t> ref_level;
+  std::vector<uint64_t> ref_per_level;
 
   uint32_t fanin_count(uint32_t e) const { return fi_off[e + 1] - fi_off[e]; }
 };

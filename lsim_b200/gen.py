@@ -128,3 +128,130 @@ def serve_configs(n_circuits=32, seed=0, gates=(1000, 500000), levels=(20, 150))
         out.append(dict(n_gates=g, n_pi=io, n_po=io, n_levels=lv, p_fanin3=0.6,
                         seed=seed * 100003 + 5000 + i, faults="collapsed"))
     return out
+
+
+def opentimer_dump(n_cells, n_pi, seed=0, loops=0, window=8, fanout_free=False, layers=None,
+                   cell_types=None):
+    """Seeded OpenTimer-style netlist dump (the input of
+    lsim_b200.opentimer.convert) over the cells of its pin table.
+
+    Cells are created in order; each input comes from a PI or an earlier
+    cell, drawn from the last ``window`` signals with probability 0.8, so
+    that paths are deep.  ``fanout_free``: every signal drives at most one
+    sink (the PI count bounds the cell count).  ``layers``: cells spread
+    over that many layers, every input from the layer just before (layer 0
+    being the PIs).  ``loops``: that many cells take one input -- a DFF's D,
+    or the last input of a multi-input cell -- from a later cell (in
+    ``layers`` mode from a later layer), which closes a cycle or adds an
+    edge against the creation order.  Every signal left without a sink
+    drives its own PO.  Names are fixed-width (pi*, po*, g*) so that no name
+    is a prefix of another.  Edges, including the arcs inside each cell, are
+    listed in a seeded random order."""
+    import numpy as np
+    from .opentimer import PIN_TABLE
+    rng = np.random.default_rng(seed)
+    kinds = sorted(PIN_TABLE) if cell_types is None else list(cell_types)
+    lib = {}
+    for k in kinds:
+        pins = PIN_TABLE[k]
+        ins = sorted((p for p in pins if pins[p] > 0), key=lambda p: pins[p])
+        out = next(p for p in pins if pins[p] == 0)
+        lib[k] = (k if k.endswith("X1") else k + "_X1", ins, out)
+    pis = ["pi%05d" % i for i in range(n_pi)]
+    cells = []  # (name, kind, [signal per input pin, None = loop input])
+    layer_of = []
+    sig = [(p, p) for p in pis]  # (source name in edges, element name)
+    pool = list(range(len(sig)))  # signals without a sink (fanout-free mode)
+    if layers:
+        bounds = [0, n_pi] + [n_pi + (n_cells * (l + 1)) // layers for l in range(layers)]
+    n_loop = 0
+    for c in range(n_cells):
+        name = "g%06d" % c
+        kind = kinds[int(rng.integers(len(kinds)))]
+        if fanout_free and len(pool) < len(lib[kind][1]) + (n_loop < loops):
+            fits = [k for k in kinds if len(lib[k][1]) <= len(pool)]
+            if not fits:
+                break
+            kind = fits[int(rng.integers(len(fits)))]
+        n_in = len(lib[kind][1])
+        want_loop = n_loop < loops and n_in >= 2 and rng.random() < 0.5
+        src = []
+        if layers:
+            lay = next(l for l in range(layers) if n_pi + c < bounds[l + 2])
+            lo, hi = bounds[lay], bounds[lay + 1]
+            for _ in range(n_in):
+                j = lo + int(rng.integers(hi - lo))
+                while j in src and hi - lo > len(src):
+                    j = lo + (j - lo + 1) % (hi - lo)
+                src.append(j)
+            want_loop = want_loop and lay + 1 < layers
+            layer_of.append(lay)
+        elif fanout_free:
+            for _ in range(n_in):
+                j = int(rng.integers(len(pool)))
+                src.append(pool[j])
+                pool[j] = pool[-1]
+                pool.pop()
+        else:
+            for _ in range(n_in):
+                if rng.random() < 0.8:
+                    j = len(sig) - 1 - int(rng.integers(min(window, len(sig))))
+                else:
+                    j = int(rng.integers(len(sig)))
+                while j in src:
+                    j = (j + 1) % len(sig)
+                src.append(j)
+        if want_loop and c + 1 < n_cells:
+            k = 0 if kind == "DFF" else n_in - 1
+            if fanout_free:
+                pool.append(src[k])
+            src[k] = None
+            n_loop += 1
+        cells.append((name, kind, src))
+        sig.append((name + ":" + lib[kind][2], name))
+        pool.append(len(sig) - 1)
+    used = set(s for _, _, src in cells for s in src if s is not None)
+    for ci, (name, kind, src) in enumerate(cells):
+        for k, s in enumerate(src):
+            if s is not None:
+                continue
+            if layers:
+                first = bounds[layer_of[ci] + 2] - n_pi
+                cand = list(range(n_pi + first, n_pi + len(cells)))
+            else:
+                cand = list(range(n_pi + ci + 1, n_pi + len(cells)))
+            if fanout_free:
+                cand = [x for x in cand if x not in used]
+            if not cand:  # no later cell free: a PI of its own
+                pis.append("pi%05d" % len(pis))
+                sig.append((pis[-1], pis[-1]))
+                cand = [len(sig) - 1]
+            s = cand[int(rng.integers(len(cand)))]
+            src[k] = s
+            used.add(s)
+    # ids: PIs first (added PIs renumber nothing: sig keeps its indices)
+    po_src = [s for s in range(len(sig)) if s not in used and ":" in sig[s][0]]
+    pos = ["po%05d" % i for i in range(len(po_src))]
+    edges = []
+    for name, kind, src in cells:
+        _, ins, out = lib[kind]
+        for pin, s in zip(ins, src):
+            edges.append((sig[s][0], name + ":" + pin))
+            if not (kind == "DFF" and pin == "D"):
+                edges.append((name + ":" + pin, name + ":" + out))
+    for po, s in zip(pos, po_src):
+        edges.append((sig[s][0], po))
+    order = rng.permutation(len(edges))
+    lines = ["module top;", "// Start PIs"] + ["input %s;" % p for p in pis] + [""]
+    lines += ["// Start POs"] + ["output %s;" % p for p in pos] + [""]
+    lines += ["// Start wires"] + ["wire n%s;" % name[1:] for name, _, _ in cells] + [""]
+    lines += ["// Start cells"]
+    for name, kind, src in cells:
+        cell, ins, out = lib[kind]
+        conn = ", ".join([".%s(%s)" % (p, sig[s][1]) for p, s in zip(ins, src)] +
+                         [".%s(n%s)" % (out, name[1:])])
+        lines.append("%s %s ( %s );" % (cell, name, conn))
+    lines += ["endmodule", "", "digraph TimingGraph {"]
+    lines += ['  "%s" -> "%s";' % edges[i] for i in order]
+    lines += ["}", ""]
+    return "\n".join(lines)
