@@ -117,6 +117,32 @@ int fsimb_load_buffers(fsimb_handle* h, const char* ckt, size_t ckt_len, const c
                        size_t flst_len, const char* ptn, size_t ptn_len);
 /* Circuit only (clears faults and patterns). */
 int fsimb_load_circuit(fsimb_handle* h, const char* ckt, size_t ckt_len);
+
+/* Circuit loader used by the three calls above.  FSIMB_LOAD_AUTO (the
+ * default): on a handle with a device, .ckt texts of 4 MiB and more are
+ * levelized on the device, smaller ones by the host reader;
+ * FSIMB_LOAD_HOST: always the host reader; FSIMB_LOAD_DEVICE: the device
+ * loader whenever the handle has a device.  The device loader tokenizes on
+ * `threads` host threads (0: the hardware threads, at most 32) and builds
+ * the element order, levels and CSRs on the device; its netlist is the
+ * host reader's, and it hands every text the host reader rejects (and
+ * netlists whose levels are not sorted in element order) back to that
+ * reader, so errors and their messages do not change.  Replaces the
+ * istream parsing and Kahn sort of _read_graph (fsim/simulation.cpp:664-941). */
+#define FSIMB_LOAD_AUTO 0
+#define FSIMB_LOAD_HOST 1
+#define FSIMB_LOAD_DEVICE 2
+int fsimb_set_loader(fsimb_handle* h, int mode, int threads);
+
+/* How the last circuit was loaded. */
+typedef struct {
+  uint32_t on_device;     /* 1: built by the device loader */
+  uint32_t handed_back;   /* 1: the device loader handed the text to the host reader */
+  uint32_t threads;       /* tokenizer threads (1 for the host reader) */
+  uint32_t waves;         /* element-order waves: longest path from the PIs + 1 */
+  double ms_total, ms_tokenize, ms_device;
+} fsimb_load_info;
+int fsimb_get_load_info(const fsimb_handle* h, fsimb_load_info* out);
 /* Faults by topological index: pin 0 = output, k = k-th input; value 0/1.
  * Replaces _read_fault (fsim/simulation.cpp:943-959) for callers that hold
  * the list in memory; input-pin faults have no reference representation. */

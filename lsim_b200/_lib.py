@@ -62,6 +62,17 @@ class Stats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class LoadInfo(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_uint32) for n in ["on_device", "handed_back", "threads", "waves"]] +
+                [(n, ctypes.c_double) for n in ["ms_total", "ms_tokenize", "ms_device"]])
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+LOAD_AUTO, LOAD_HOST, LOAD_DEVICE = 0, 1, 2
+
+
 class GenConfig(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("seed", ctypes.c_uint64),
                 ("n_gates", ctypes.c_uint32), ("n_pi", ctypes.c_uint32),
@@ -160,6 +171,8 @@ SIGNATURES = {
     "fsimb_found_fault_to_pattern": (ctypes.c_int, [_P, _U64P, _U64]),
     "fsimb_good_values": (ctypes.c_int, [_P, _U64, _U64P, _U64]),
     "fsimb_get_info": (ctypes.c_int, [_P, ctypes.POINTER(Info)]),
+    "fsimb_set_loader": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
+    "fsimb_get_load_info": (ctypes.c_int, [_P, ctypes.POINTER(LoadInfo)]),
     "fsimb_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
     "fsimb_topo_map": (ctypes.c_int, [_P, _U64P, _U64]),
     "fsimb_levels": (ctypes.c_int, [_P, _U64P, _U64]),

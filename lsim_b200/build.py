@@ -17,8 +17,9 @@ LIB = os.path.join(HERE, "libfsimb200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 CXX_SOURCES = ["fsimb_netlist.cpp", "fsimb_gen.cpp", "fsimb_plan.cpp"]
-CU_SOURCES = ["fsimb_kernels.cu", "fsimb_engine.cu", "fsimb_batch.cu", "fsimb_serve.cu"]
-HEADERS = ["fsimb_netlist.h", "fsimb_gen.h", "fsimb_plan.h", "fsimb_kernels.cuh", "fsimb_internal.h", "fsimb_batch.h"]
+CU_SOURCES = ["fsimb_kernels.cu", "fsimb_engine.cu", "fsimb_batch.cu", "fsimb_serve.cu", "fsimb_loader.cu"]
+HEADERS = ["fsimb_netlist.h", "fsimb_gen.h", "fsimb_plan.h", "fsimb_kernels.cuh", "fsimb_internal.h", "fsimb_batch.h",
+           "fsimb_loader.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 APPS = ["fsimb_simple", "fsimb_ma_partition"]  # drop-ins for main/simple and MA_cuda_partition
 BIN = os.path.join(HERE, "bin")

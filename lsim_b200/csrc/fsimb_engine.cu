@@ -823,6 +823,32 @@ int fsimb_get_info(const fsimb_handle* hc, fsimb_info* out) {
   API_END(h)
 }
 
+int fsimb_set_loader(fsimb_handle* h, int mode, int threads) {
+  API_BEGIN(h)
+  if (mode < FSIMB_LOAD_AUTO || mode > FSIMB_LOAD_DEVICE) throw ArgError{"loader mode must be 0, 1 or 2"};
+  if (threads < 0 || threads > 1024) throw ArgError{"loader threads must be 0..1024"};
+  h->load_mode = mode;
+  h->load_threads = threads;
+  API_END(h)
+}
+
+int fsimb_get_load_info(const fsimb_handle* hc, fsimb_load_info* out) {
+  fsimb_handle* h = const_cast<fsimb_handle*>(hc);
+  API_BEGIN(h)
+  if (!out) throw ArgError{"null output"};
+  if (!h->has_ckt) throw StateError{"no circuit loaded"};
+  const LoadInfo& li = h->load_info;
+  *out = fsimb_load_info{};
+  out->on_device = li.on_device;
+  out->handed_back = li.handed_back;
+  out->threads = (uint32_t)li.threads;
+  out->waves = li.waves;
+  out->ms_total = li.ms_total;
+  out->ms_tokenize = li.ms_tokenize;
+  out->ms_device = li.ms_device;
+  API_END(h)
+}
+
 int fsimb_get_stats(const fsimb_handle* hc, fsimb_stats* out) {
   fsimb_handle* h = const_cast<fsimb_handle*>(hc);
   API_BEGIN(h)

@@ -7,12 +7,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <functional>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/fsimb.h"
+#include "fsimb_loader.h"
 #include "fsimb_netlist.h"
 #include "fsimb_plan.h"
 
@@ -254,9 +256,24 @@ struct fsimb_handle {
     good_tiles = 0;
   }
 
+  // Circuit loader (fsimb_set_loader): 0 automatic, 1 host, 2 device.
+  int load_mode = 0;
+  int load_threads = 0;
+  fsimb::LoadInfo load_info;
+
   void load_ckt(const char* t, size_t n) {
     fsimb::Netlist tmp;
-    fsimb::parse_ckt(t, n, tmp);
+    const bool dev = device >= 0 && (load_mode == 2 || (load_mode == 0 && n >= fsimb::kDeviceLoadBytes));
+    const auto t0 = std::chrono::steady_clock::now();
+    fsimb::LoadInfo li;
+    if (!dev || !fsimb::parse_ckt_device(t, n, tmp, device, stream, load_threads, li)) {
+      fsimb::parse_ckt(t, n, tmp);
+      li = fsimb::LoadInfo{};
+      li.handed_back = dev;
+      li.threads = 1;
+      li.ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    load_info = li;
     nl = std::move(tmp);
     has_ckt = true;
     gen = plan_gen = fsimb::next_generation();

@@ -86,6 +86,19 @@ class Simulator:
                                                   b[2], len(b[2])))
         self._ran = False
 
+    def set_loader(self, mode="auto", threads=0):
+        """Circuit loader for the reads that follow: "auto" (device loader for
+        texts of 4 MiB and more on a device handle), "host" or "device"."""
+        m = {"auto": _lib.LOAD_AUTO, "host": _lib.LOAD_HOST, "device": _lib.LOAD_DEVICE}[mode]
+        self._check(_lib.lib().fsimb_set_loader(self._h, m, int(threads)))
+
+    def load_info(self):
+        """How the last circuit was loaded (on_device, handed_back, threads,
+        waves, ms_total, ms_tokenize, ms_device)."""
+        li = _lib.LoadInfo()
+        self._check(_lib.lib().fsimb_get_load_info(self._h, ctypes.byref(li)))
+        return li.as_dict()
+
     def load_circuit(self, ckt):
         b = ckt.encode() if isinstance(ckt, str) else bytes(ckt)
         self._check(_lib.lib().fsimb_load_circuit(self._h, b, len(b)))
