@@ -352,7 +352,8 @@ int fsimb_server_create(int device, const fsimb_server_opts* opts, fsimb_server*
 /* Finishes the requests in flight, then frees everything. */
 int fsimb_server_destroy(fsimb_server* s);
 const char* fsimb_server_last_error(const fsimb_server* s);
-/* Circuit text (.ckt) and an optional resident pattern block [ceil(P/64)][nPI]. */
+/* Circuit text (.ckt) and an optional resident pattern block [ceil(P/64)][nPI].
+ * Texts of 4 MiB and more are loaded by the device loader (fsimb_set_loader). */
 int fsimb_server_add_circuit(fsimb_server* s, const char* ckt, size_t ckt_len, const uint64_t* words,
                              uint64_t n_patterns, uint32_t* id);
 int fsimb_server_submit(fsimb_server* s, const fsimb_request* req, uint64_t* ticket);

@@ -237,7 +237,21 @@ struct fsimb_server {
 
   uint32_t add_circuit(const char* ckt, size_t len, const uint64_t* words, uint64_t n_patterns) {
     auto c = std::make_unique<ResidentCircuit>();
-    parse_ckt(ckt, len, c->nl);
+    bool loaded = false;
+    if (len >= kDeviceLoadBytes) {  // large circuits: the device loader, on a stream of its own
+      CK(cudaSetDevice(device));
+      cudaStream_t ls;
+      CK(cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking));
+      LoadInfo li;
+      try {
+        loaded = parse_ckt_device(ckt, len, c->nl, device, ls, 0, li);
+      } catch (...) {
+        cudaStreamDestroy(ls);
+        throw;
+      }
+      cudaStreamDestroy(ls);
+    }
+    if (!loaded) parse_ckt(ckt, len, c->nl);
     const Netlist& nl = c->nl;
     if (n_patterns && !words) throw ArgError{"null pattern words"};
     c->block.P = n_patterns;
