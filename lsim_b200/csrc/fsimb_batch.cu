@@ -837,10 +837,155 @@ struct fsimb_batch {
     return js;
   }
 
+  // One timed sweep launch of class 0 of `tx` (work counters reset first);
+  // the fastest of two runs, after an untimed one when `warm`.
+  float time_class0(BatchExec& tx, bool warm, cudaStream_t s) {
+    cudaEvent_t e0 = ev(0), e1 = ev(1);
+    float ms = 1e30f;
+    for (int rep = warm ? -1 : 0; rep < 2; ++rep) {
+      CK(cudaMemsetAsync(tx.d_ctl.p, 0, tx.ctl_bytes, s));
+      CK(cudaEventRecord(e0, s));
+      tx.enqueue_sweeps(s, 0);
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float x = 0;
+      CK(cudaEventElapsedTime(&x, e0, e1));
+      int kerr = 0;
+      CK(cudaMemcpy(&kerr, tx.d_ctl.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (kerr) throw CudaError{"a sweep kernel reached its wait limit during tuning"};
+      if (rep >= 0) ms = std::min(ms, x);
+    }
+    return ms;
+  }
+
+  // Members that carry at least 1% of the batch's sweep work (the largest 64
+  // at most) get a class of their own, tuned as the plain path tunes a
+  // circuit alone: words per item x CTAs per SM x CTA size (256-1,024
+  // threads), timed on every stride-th sweep of the first tile, the default
+  // shape kept unless beaten by 2%.  A shared class cannot give
+  // each of these circuits its own shape, and they carry most of the work.
+  // Returns, per class of the new assignment, whether its shape is final.
+  std::vector<char> tune_singletons(BatchAssign& a, cudaStream_t s) {
+    const size_t n = members.size();
+    std::vector<double> wall(n);
+    double total = 0;
+    for (size_t i = 0; i < n; ++i) {
+      const uint64_t tiles = std::max<uint64_t>(1, (members[i]->pats.W + kTileWords - 1) / kTileWords);
+      wall[i] = ((double)members[i]->plan.dense_sweep_gates + 1.0) * (double)tiles;
+      total += wall[i];
+    }
+    std::vector<size_t> dom;
+    for (size_t i = 0; i < n; ++i)
+      if (!members[i]->plan.sweeps.empty() && wall[i] >= 0.01 * total) dom.push_back(i);
+    std::sort(dom.begin(), dom.end(), [&](size_t x, size_t y) { return wall[x] > wall[y]; });
+    if (dom.size() > 64) dom.resize(64);
+    if (dom.empty()) return std::vector<char>(a.shapes.size(), 0);
+
+    std::vector<ClassShape> chosen(dom.size());
+    bool warm = true;
+    for (size_t d = 0; d < dom.size(); ++d) {
+      const size_t i = dom[d];
+      const Plan& P = members[i]->plan;
+      const uint32_t ns = (uint32_t)P.sweeps.size();
+      // about 1,024 sweeps: with up to 64 such circuits a quarter of the
+      // plain tuner's sample keeps the whole search to seconds
+      const uint32_t stride = std::max<uint32_t>(1, ns / 1024);
+      Plan ps = P;  // the sample: every stride-th sweep (timing only)
+      ps.sweeps.clear();
+      for (uint32_t q = 0; q < ns; q += stride) ps.sweeps.push_back(P.sweeps[q]);
+      const ClassShape def = a.shapes[a.cls[i]];
+      ClassShape best = def;
+      float best_ms = 1e30f;
+      bool best_is_default = false;
+      std::vector<int> Ms{def.M};
+      for (int m : {8, 4, 2, 1})
+        if (m != def.M) Ms.push_back(m);
+      const size_t share1 = smem_share(1);
+      for (int M : Ms) {
+        if (sweep_vals_bytes(P.max_live, M) > share1) continue;
+        const Schedule& sc = schedule_at(i, M);
+        if (sc.max_live > kMaxSlots || sweep_vals_bytes(sc.max_live, M) > share1) continue;
+        BatchJob j;
+        j.nl = &members[i]->nl;
+        j.plan = &ps;
+        j.sched = &sc;
+        j.pats = &members[i]->pats;
+        j.F = members[i]->faults.size();
+        j.M = M;
+        j.cls = 0;
+        BatchExec tx;
+        tx.n_sms = n_sms;
+        tx.smem_optin = smem_optin;
+        tx.smem_per_sm = smem_per_sm;
+        tx.layout({j}, {ClassShape{M, 256, 1}}, true, s);
+        tx.enqueue(s, true, false, nullptr);  // good machine of the first tile
+        SweepClass& kc = tx.classes[0];
+        std::vector<ClassShape> cands;
+        if (M == def.M) cands.push_back(def);
+        for (int occ : {1, 2, 3, 4})
+          for (int T : {256, 384, 512, 768, 1024})
+            if (T <= (int)sweep_max_threads(M) && T * occ <= 2048 &&
+                !(M == def.M && occ == def.occ && T == def.threads))
+              cands.push_back(ClassShape{M, T, occ});
+        for (const ClassShape& sh : cands) {
+          if (sweep_vals_bytes(sc.max_live, M) > smem_share(sh.occ)) continue;
+          try {
+            tx.size_class(kc, sh);
+          } catch (const LimitError&) {
+            continue;
+          }
+          if (sh.occ > 1 && kc.rec_buf < std::min<uint32_t>(kc.widest, 64)) continue;
+          if (kc.blocks < (int)std::min<unsigned long long>((unsigned long long)n_sms * sh.occ, kc.n_items))
+            continue;  // fewer CTAs per SM than asked: the same as a smaller shape
+          const float ms = time_class0(tx, warm, s);
+          warm = false;
+          const bool is_default = sh.M == def.M && sh.occ == def.occ && sh.threads == def.threads;
+          if (is_default || ms < (best_is_default ? 0.98f : 1.0f) * best_ms) {
+            best_ms = ms;
+            best = sh;
+            best_is_default = is_default;
+          }
+        }
+        tx.release();
+      }
+      chosen[d] = best;
+    }
+
+    // New assignment: the other members keep their shared classes, each
+    // dominant member its own.
+    std::vector<char> is_dom(n, 0);
+    for (size_t i : dom) is_dom[i] = 1;
+    BatchAssign b;
+    b.M = a.M;
+    b.cls.assign(n, -1);
+    std::vector<int> remap(a.shapes.size(), -1);
+    for (size_t i = 0; i < n; ++i) {
+      if (is_dom[i]) continue;
+      int& r = remap[a.cls[i]];
+      if (r < 0) {
+        r = (int)b.shapes.size();
+        b.shapes.push_back(a.shapes[a.cls[i]]);
+      }
+      b.cls[i] = r;
+    }
+    std::vector<char> fixed(b.shapes.size(), 0);
+    for (size_t d = 0; d < dom.size(); ++d) {
+      b.cls[dom[d]] = (int)b.shapes.size();
+      b.M[dom[d]] = chosen[d].M;
+      b.shapes.push_back(chosen[d]);
+      fixed.push_back(1);
+    }
+    b.max_live.assign(b.shapes.size(), 0);
+    for (size_t i = 0; i < n; ++i)
+      b.max_live[b.cls[i]] = std::max(b.max_live[b.cls[i]], schedule_at(i, b.M[i]).max_live);
+    a = std::move(b);
+    return fixed;
+  }
+
   // Times candidate shapes per class (CTAs per SM x CTA size, words per item
   // fixed) on the first tile of a spread of the class's circuits (about 3%
   // of its sweep work); the default shape stays unless beaten by 2%.
-  void autotune(BatchAssign& a, cudaStream_t s) {
+  void autotune(BatchAssign& a, cudaStream_t s, const std::vector<char>& fixed) {
     const size_t n = members.size();
     const size_t n_cls = a.shapes.size();
     std::vector<double> w1(n), wall(n);
@@ -851,6 +996,7 @@ struct fsimb_batch {
     }
     std::vector<size_t> sample;
     for (size_t c = 0; c < n_cls; ++c) {
+      if (fixed[c]) continue;  // tuned on its own already
       std::vector<size_t> in;
       double total = 0, t0 = 0;
       for (size_t i = 0; i < n; ++i)
@@ -866,6 +1012,7 @@ struct fsimb_batch {
       if (!picked && !in.empty()) sample.push_back(in.back());
     }
     std::sort(sample.begin(), sample.end());
+    if (sample.empty()) return;
 
     BatchExec tx;
     tx.n_sms = n_sms;
@@ -970,7 +1117,8 @@ void fsimb_batch::run(const fsimb_batch_opts* opts) {
     if (!has_tuned || tuned_members != members || tuned_gens != g) {
       const auto t0 = std::chrono::steady_clock::now();
       tuned = auto_assign();
-      autotune(tuned, s);
+      const std::vector<char> fixed = tune_singletons(tuned, s);
+      autotune(tuned, s, fixed);
       tuned_members = members;
       tuned_gens = g;
       has_tuned = true;
