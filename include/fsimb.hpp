@@ -103,6 +103,16 @@ class Simulator {
     fsimb_free_text(text);
   }
 
+  /* Circuit loader for the reads that follow (FSIMB_LOAD_AUTO / _HOST /
+   * _DEVICE, tokenizer threads; fsimb_set_loader) and how the last circuit
+   * was loaded. */
+  void set_loader(int mode, int threads = 0) { check(fsimb_set_loader(h_, mode, threads)); }
+  fsimb_load_info load_info() const {
+    fsimb_load_info li{};
+    check(fsimb_get_load_info(h_, &li));
+    return li;
+  }
+
   fsimb_handle* handle() { return h_; }
 
  private:
