@@ -837,12 +837,12 @@ struct fsimb_batch {
     return js;
   }
 
-  // One timed sweep launch of class 0 of `tx` (work counters reset first);
-  // the fastest of two runs, after an untimed one when `warm`.
-  float time_class0(BatchExec& tx, bool warm, cudaStream_t s) {
+  // Sweep time of class 0 of `tx` (work counters reset before each run):
+  // the fastest of `runs` runs, after an untimed one when `warm`.
+  float time_class0(BatchExec& tx, bool warm, cudaStream_t s, int runs) {
     cudaEvent_t e0 = ev(0), e1 = ev(1);
     float ms = 1e30f;
-    for (int rep = warm ? -1 : 0; rep < 2; ++rep) {
+    for (int rep = warm ? -1 : 0; rep < runs; ++rep) {
       CK(cudaMemsetAsync(tx.d_ctl.p, 0, tx.ctl_bytes, s));
       CK(cudaEventRecord(e0, s));
       tx.enqueue_sweeps(s, 0);
@@ -860,9 +860,10 @@ struct fsimb_batch {
 
   // Members that carry at least 1% of the batch's sweep work (the largest 64
   // at most) get a class of their own, tuned as the plain path tunes a
-  // circuit alone: words per item x CTAs per SM x CTA size (256-1,024
-  // threads), timed on every stride-th sweep of the first tile, the default
-  // shape kept unless beaten by 2%.  A shared class cannot give
+  // circuit alone over words per item x CTAs per SM x CTA size (256-1,024
+  // threads), on strided samples of the first tile's sweeps: every
+  // candidate once on about 256 sweeps, then the default and the three
+  // fastest twice on about 1,024, the default kept unless beaten by 2%.  A shared class cannot give
   // each of these circuits its own shape, and they carry most of the work.
   // Returns, per class of the new assignment, whether its shape is final.
   std::vector<char> tune_singletons(BatchAssign& a, cudaStream_t s) {
@@ -887,57 +888,89 @@ struct fsimb_batch {
       const size_t i = dom[d];
       const Plan& P = members[i]->plan;
       const uint32_t ns = (uint32_t)P.sweeps.size();
-      // about 1,024 sweeps: with up to 64 such circuits a quarter of the
-      // plain tuner's sample keeps the whole search to seconds
-      const uint32_t stride = std::max<uint32_t>(1, ns / 1024);
-      Plan ps = P;  // the sample: every stride-th sweep (timing only)
-      ps.sweeps.clear();
-      for (uint32_t q = 0; q < ns; q += stride) ps.sweeps.push_back(P.sweeps[q]);
+      // Two samples: every stride-th sweep, about 256 (coarse) and about
+      // 1,024 (fine) of them (timing only).
+      Plan coarse = P, fine = P;
+      for (Plan* q : {&coarse, &fine}) {
+        const uint32_t stride = std::max<uint32_t>(1, ns / (q == &coarse ? 256u : 1024u));
+        q->sweeps.clear();
+        for (uint32_t k = 0; k < ns; k += stride) q->sweeps.push_back(P.sweeps[k]);
+      }
       const ClassShape def = a.shapes[a.cls[i]];
-      ClassShape best = def;
-      float best_ms = 1e30f;
-      bool best_is_default = false;
-      std::vector<int> Ms{def.M};
-      for (int m : {8, 4, 2, 1})
-        if (m != def.M) Ms.push_back(m);
       const size_t share1 = smem_share(1);
-      for (int M : Ms) {
-        if (sweep_vals_bytes(P.max_live, M) > share1) continue;
+      auto fits_M = [&](int M) {
+        if (sweep_vals_bytes(P.max_live, M) > share1) return false;
         const Schedule& sc = schedule_at(i, M);
-        if (sc.max_live > kMaxSlots || sweep_vals_bytes(sc.max_live, M) > share1) continue;
+        return sc.max_live <= kMaxSlots && sweep_vals_bytes(sc.max_live, M) <= share1;
+      };
+      // A one-circuit layout of `plan` at M, with its first tile's good machine.
+      auto lay = [&](BatchExec& tx, const Plan& plan, int M) {
         BatchJob j;
         j.nl = &members[i]->nl;
-        j.plan = &ps;
-        j.sched = &sc;
+        j.plan = &plan;
+        j.sched = &schedule_at(i, M);
         j.pats = &members[i]->pats;
         j.F = members[i]->faults.size();
         j.M = M;
         j.cls = 0;
-        BatchExec tx;
         tx.n_sms = n_sms;
         tx.smem_optin = smem_optin;
         tx.smem_per_sm = smem_per_sm;
         tx.layout({j}, {ClassShape{M, 256, 1}}, true, s);
-        tx.enqueue(s, true, false, nullptr);  // good machine of the first tile
+        tx.enqueue(s, true, false, nullptr);
+      };
+      // Sizes class 0 of tx at sh; false if the shape does not run as asked.
+      auto usable = [&](BatchExec& tx, const ClassShape& sh) {
+        if (sweep_vals_bytes(schedule_at(i, sh.M).max_live, sh.M) > smem_share(sh.occ)) return false;
         SweepClass& kc = tx.classes[0];
-        std::vector<ClassShape> cands;
-        if (M == def.M) cands.push_back(def);
+        try {
+          tx.size_class(kc, sh);
+        } catch (const LimitError&) {
+          return false;
+        }
+        if (sh.occ > 1 && kc.rec_buf < std::min<uint32_t>(kc.widest, 64)) return false;
+        // fewer CTAs per SM than asked: the same as a smaller shape
+        return kc.blocks >= (int)std::min<unsigned long long>((unsigned long long)n_sms * sh.occ, kc.n_items);
+      };
+      // Stage 1: every candidate once on the coarse sample.
+      struct Timed {
+        float ms;
+        ClassShape sh;
+      };
+      std::vector<Timed> t1;
+      for (int M : {8, 4, 2, 1}) {
+        if (!fits_M(M)) continue;
+        BatchExec tx;
+        lay(tx, coarse, M);
         for (int occ : {1, 2, 3, 4})
-          for (int T : {256, 384, 512, 768, 1024})
-            if (T <= (int)sweep_max_threads(M) && T * occ <= 2048 &&
-                !(M == def.M && occ == def.occ && T == def.threads))
-              cands.push_back(ClassShape{M, T, occ});
-        for (const ClassShape& sh : cands) {
-          if (sweep_vals_bytes(sc.max_live, M) > smem_share(sh.occ)) continue;
-          try {
-            tx.size_class(kc, sh);
-          } catch (const LimitError&) {
-            continue;
+          for (int T : {256, 384, 512, 768, 1024}) {
+            const ClassShape sh{M, T, occ};
+            if (T > (int)sweep_max_threads(M) || T * occ > 2048 || !usable(tx, sh)) continue;
+            t1.push_back(Timed{time_class0(tx, warm, s, 1), sh});
+            warm = false;
           }
-          if (sh.occ > 1 && kc.rec_buf < std::min<uint32_t>(kc.widest, 64)) continue;
-          if (kc.blocks < (int)std::min<unsigned long long>((unsigned long long)n_sms * sh.occ, kc.n_items))
-            continue;  // fewer CTAs per SM than asked: the same as a smaller shape
-          const float ms = time_class0(tx, warm, s);
+        tx.release();
+      }
+      std::sort(t1.begin(), t1.end(), [](const Timed& x, const Timed& y) { return x.ms < y.ms; });
+      // Stage 2: the default and the three fastest, twice each on the fine
+      // sample; the default stays unless beaten by 2%.
+      std::vector<ClassShape> fin{def};
+      for (const Timed& t : t1) {
+        if (fin.size() >= 4) break;
+        if (!(t.sh.M == def.M && t.sh.occ == def.occ && t.sh.threads == def.threads)) fin.push_back(t.sh);
+      }
+      ClassShape best = def;
+      float best_ms = 1e30f;
+      bool best_is_default = false;
+      for (int M : {8, 4, 2, 1}) {
+        bool any = false;
+        for (const ClassShape& sh : fin) any |= sh.M == M;
+        if (!any || !fits_M(M)) continue;
+        BatchExec tx;
+        lay(tx, fine, M);
+        for (const ClassShape& sh : fin) {
+          if (sh.M != M || !usable(tx, sh)) continue;
+          const float ms = time_class0(tx, warm, s, 2);
           warm = false;
           const bool is_default = sh.M == def.M && sh.occ == def.occ && sh.threads == def.threads;
           if (is_default || ms < (best_is_default ? 0.98f : 1.0f) * best_ms) {
