@@ -135,11 +135,13 @@ def _walk_reference(sinks, pis, po_set, mode, warnings):
             if cur not in po_set and warnings is not None:
                 warnings.append("no connection found for %s" % cur)
             continue
-        for out in [x.split(":")[0] for x in sinks[key]]:
-            if out in taken:
-                sinks[key] = [x for x in sinks[key] if x.split(":")[0] != out]
-            else:
-                todo.append(out)
+        # `taken` does not change while one element's sinks are looked at, so
+        # the reference's removal per taken sink element is one pass here
+        outs = [x.split(":")[0] for x in sinks[key]]
+        drop = {out for out in outs if out in taken}
+        if drop:
+            sinks[key] = [x for x, out in zip(sinks[key], outs) if out not in drop]
+        todo.extend(out for out in outs if out not in taken)
 
 
 def _walk_loops(sinks, listing):
@@ -213,13 +215,13 @@ def convert(text, mode="bfs", pin_table=None, strict=False, warnings=None):
     types = [gate_type(ctype, warnings) for _, ctype in cells]
 
     # driving pin -> sinks, in dump order, each sink once (fsim/parser.py:94-102)
-    sinks = {}
+    sinks, seen = {}, set()
     for src, dst in edges:
         if src.split(":")[0] == dst.split(":")[0]:
             continue  # an arc inside one cell
-        lst = sinks.setdefault(src, [])
-        if dst not in lst:
-            lst.append(dst)
+        if (src, dst) not in seen:
+            seen.add((src, dst))
+            sinks.setdefault(src, []).append(dst)
 
     if mode == "loops":
         _walk_loops(sinks, pis + [c[0] for c in cells] + pos)

@@ -151,6 +151,27 @@ def test_bfs_keeps_exactly_the_edges_into_the_next_layer():
     assert kept == want
 
 
+def test_high_fanout_net_whose_sinks_were_all_taken():
+    """A clock buffer reached after the 30,000 flip-flops it drives loses all
+    of its edges in bfs mode; the removals take one pass over its sinks, not
+    one pass per sink."""
+    n = 30000
+    lines = ["module top;", "// Start PIs", "input clk;", "input d;", "", "// Start POs"]
+    lines += ["output po%05d;" % i for i in range(n)] + ["", "// Start wires", "", "// Start cells",
+                                                        "INV_X1 i0 ( );", "INV_X1 i1 ( );",
+                                                        "CLKBUF_X1 b0 ( );"]
+    lines += ["DFF_X1 f%05d ( );" % i for i in range(n)] + ["endmodule", "", "digraph TimingGraph {"]
+    lines += ['  "clk" -> "i0:A";', '  "i0:ZN" -> "i1:A";', '  "i1:ZN" -> "b0:A";']
+    for i in range(n):
+        lines += ['  "b0:Z" -> "f%05d:CK";' % i, '  "d" -> "f%05d:D";' % i,
+                  '  "f%05d:Q" -> "po%05d";' % (i, i)]
+    ckt = opentimer.convert("\n".join(lines + ["}", ""]), "bfs")
+    w = dict(wires_of(ckt))
+    b0 = 2 + n + 2  # ids: clk d, POs, i0 i1 b0, flip-flops
+    assert w[(b0, 0)] == []
+    assert len(w[(1, 0)]) == n and all(pin == 1 for _, pin in w[(1, 0)])
+
+
 def test_tables_and_errors():
     assert opentimer.gate_type("NAND2_X1") == 4 and opentimer.gate_type("XNOR2_X1") == 6
     assert opentimer.gate_type("AOI22_X2") == 4 and opentimer.gate_type("OAI21_X1") == 5
