@@ -68,3 +68,32 @@ def test_oracle_matches_reference_when_rounds_exceed_pis():
     o = Oracle(w["ckt"], w["flst"], w["ptn"])
     ref = Reference(w["ckt"], w["flst"], words=o.words, P=o.P, n_pi=o.n_pi)
     assert np.array_equal(o.simulate(), ref.simulate())
+
+
+@needs_ref
+def test_oracle_matches_reference_on_seeded_random_circuits():
+    """48 small circuits drawn from one seed: every gate type (MUX included),
+    fan-in up to 3, 1-4 levels back, partial last rounds, one to five
+    rounds, output faults, at most as many POs as gates; also the
+    reference's last-round table and good values."""
+    rng = np.random.default_rng(2024)
+    for case in range(48):
+        n_gates = int(rng.integers(5, 400))
+        n_pi = int(rng.integers(1, 24))
+        # more POs than gates would drive a PO from a PI, where the reference
+        # writes past its gate array (fsim/simulation.cpp:856-861)
+        n_po = int(rng.integers(1, min(16, n_gates) + 1))
+        n_levels = int(rng.integers(1, max(2, min(n_gates, 30))))
+        P = int(rng.integers(1, 64 * min(5, n_pi) + 1))  # ceil(P/64) <= nPI: defined row placement
+        mask = gen.ALL_TYPES if case % 2 else gen.BENCH_TYPES
+        w = gen.generate(n_gates=n_gates, n_pi=n_pi, n_po=n_po, n_levels=n_levels, n_patterns=P,
+                         type_mask=mask, seed=1000 + case, faults="outputs",
+                         window=int(rng.integers(1, 5)))
+        o = Oracle(w["ckt"], w["flst"], w["ptn"])
+        ref = Reference(w["ckt"], w["flst"], w["ptn"])
+        assert np.array_equal(o.simulate(), ref.simulate()), case
+        table, good = ref.run_table(mode=0)
+        r = o.simulate()
+        assert list(table[0::2]) == list(r["ref_flag"]), case
+        assert list(table[1::2]) == list(r["ref_rd"]), case
+        assert list(good) == list(o.good_values()), case
