@@ -227,3 +227,36 @@ def test_fault_costs_group_faults_that_share_a_sweep():
         _, first = np.unique(group[idx], return_index=True)
         loads.append(float(cost[idx][first].sum()))
     assert max(loads) <= 1.2 * min(loads) + cost.max()      # balanced
+
+
+def test_shard_partitions_cover_everything_once():
+    """Pattern blocks are contiguous, cut at 2,048-pattern tiles, disjoint and
+    cover every round (ranks past the last tile get none); fault parts keep
+    each sweep group on one rank and are balanced within the largest
+    group's cost."""
+    from lsim_b200 import shard
+    for n_rounds in (1, 31, 32, 33, 1024, 1000):
+        for world in (1, 2, 3, 4, 8, 64):
+            blocks = [shard.round_block(n_rounds, r, world) for r in range(world)]
+            at = 0
+            for r0, r1 in blocks:
+                if r1 > r0:  # an empty block may sit anywhere
+                    assert r0 == at and r0 % 32 == 0 and (r1 % 32 == 0 or r1 == n_rounds)
+                at = max(at, r1)
+            assert at == n_rounds
+            assert sum(r1 - r0 for r0, r1 in blocks) == n_rounds
+    rng = np.random.default_rng(5)
+    group = rng.integers(0, 300, size=5000)
+    cost = rng.integers(1, 1000, size=5000)
+    for world in (1, 2, 3, 8):
+        parts = shard.split_faults(group, cost, world)
+        allidx = np.concatenate(parts)
+        assert len(allidx) == 5000 and len(np.unique(allidx)) == 5000
+        owner = np.empty(5000, dtype=np.int64)
+        for r, p in enumerate(parts):
+            owner[p] = r
+        for g in np.unique(group):
+            assert len(np.unique(owner[group == g])) == 1
+        gcost = {g: cost[group == g].max() for g in np.unique(group)}
+        load = [sum(gcost[g] for g in np.unique(group[p])) for p in parts]
+        assert max(load) - min(load) <= max(gcost.values())
