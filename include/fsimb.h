@@ -126,8 +126,9 @@ int fsimb_load_circuit(fsimb_handle* h, const char* ckt, size_t ckt_len);
  * `threads` host threads (0: the hardware threads, at most 32) and builds
  * the element order, levels and CSRs on the device; its netlist is the
  * host reader's, and it hands every text the host reader rejects (and
- * netlists whose levels are not sorted in element order) back to that
- * reader, so errors and their messages do not change.  Replaces the
+ * netlists whose levels are not sorted in element order, and texts it
+ * finds no device memory for) back to that reader, so errors and their
+ * messages do not change.  Replaces the
  * istream parsing and Kahn sort of _read_graph (fsim/simulation.cpp:664-941). */
 #define FSIMB_LOAD_AUTO 0
 #define FSIMB_LOAD_HOST 1

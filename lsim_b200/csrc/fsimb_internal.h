@@ -266,7 +266,18 @@ struct fsimb_handle {
     const bool dev = device >= 0 && (load_mode == 2 || (load_mode == 0 && n >= fsimb::kDeviceLoadBytes));
     const auto t0 = std::chrono::steady_clock::now();
     fsimb::LoadInfo li;
-    if (!dev || !fsimb::parse_ckt_device(t, n, tmp, device, stream, load_threads, li)) {
+    bool built = false;
+    if (dev) {
+      try {
+        built = fsimb::parse_ckt_device(t, n, tmp, device, stream, load_threads, li);
+      } catch (const fsimb::CudaError&) {
+        // no room on the device (or the like): the host reader still can
+        cudaStreamSynchronize(stream);
+        cudaGetLastError();
+        built = false;
+      }
+    }
+    if (!built) {
       fsimb::parse_ckt(t, n, tmp);
       li = fsimb::LoadInfo{};
       li.handed_back = dev;

@@ -245,6 +245,10 @@ struct fsimb_server {
       LoadInfo li;
       try {
         loaded = parse_ckt_device(ckt, len, c->nl, device, ls, 0, li);
+      } catch (const CudaError&) {
+        loaded = false;  // no room on the device (or the like): the host reader still can
+        cudaStreamSynchronize(ls);
+        cudaGetLastError();
       } catch (...) {
         cudaStreamDestroy(ls);
         throw;
