@@ -260,3 +260,24 @@ def test_shard_partitions_cover_everything_once():
         gcost = {g: cost[group == g].max() for g in np.unique(group)}
         load = [sum(gcost[g] for g in np.unique(group[p])) for p in parts]
         assert max(load) - min(load) <= max(gcost.values())
+
+
+def test_loader_selection_on_a_host_handle():
+    """fsimb_set_loader / fsimb_get_load_info without a GPU: a host-only
+    handle always uses the host reader, whatever mode is asked for."""
+    s = Simulator(-1)
+    with pytest.raises(FsimbError) as e:
+        s.load_info()
+    assert e.value.code == _lib.ERR_STATE
+    for bad in ((3, 0), (-1, 0), (0, -2), (0, 5000)):
+        rc = _lib.lib().fsimb_set_loader(s._h, *bad)
+        assert rc == _lib.ERR_ARG
+    w = gen.generate(n_gates=200, n_pi=8, n_po=8, n_levels=10, n_patterns=100, seed=3)
+    for mode in ("auto", "host", "device"):
+        s.set_loader(mode, 4)
+        s.load_circuit(w["ckt"])
+        li = s.load_info()
+        assert li["on_device"] == 0 and li["handed_back"] == 0 and li["threads"] == 1
+        assert li["ms_total"] >= 0
+    with pytest.raises(KeyError):
+        s.set_loader("gpu")
