@@ -131,7 +131,7 @@ def serve_configs(n_circuits=32, seed=0, gates=(1000, 500000), levels=(20, 150))
 
 
 def opentimer_dump(n_cells, n_pi, seed=0, loops=0, window=8, fanout_free=False, layers=None,
-                   cell_types=None):
+                   cell_types=None, pins=None):
     """Seeded OpenTimer-style netlist dump (the input of
     lsim_b200.opentimer.convert) over the cells of its pin table.
 
@@ -146,14 +146,16 @@ def opentimer_dump(n_cells, n_pi, seed=0, loops=0, window=8, fanout_free=False, 
     edge against the creation order.  Every signal left without a sink
     drives its own PO.  Names are fixed-width (pi*, po*, g*) so that no name
     is a prefix of another.  Edges, including the arcs inside each cell, are
-    listed in a seeded random order."""
+    listed in a seeded random order.  ``pins``: the pin table to draw cells
+    from (default: the converter's PIN_TABLE)."""
     import numpy as np
     from .opentimer import PIN_TABLE
     rng = np.random.default_rng(seed)
-    kinds = sorted(PIN_TABLE) if cell_types is None else list(cell_types)
+    table = PIN_TABLE if pins is None else pins
+    kinds = sorted(table) if cell_types is None else list(cell_types)
     lib = {}
     for k in kinds:
-        pins = PIN_TABLE[k]
+        pins = table[k]
         ins = sorted((p for p in pins if pins[p] > 0), key=lambda p: pins[p])
         out = next(p for p in pins if pins[p] == 0)
         lib[k] = (k if k.endswith("X1") else k + "_X1", ins, out)

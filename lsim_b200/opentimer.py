@@ -66,6 +66,21 @@ PIN_TABLE = {
     "NAND3X1": {"A": 1, "B": 2, "C": 3, "Y": 0},
 }
 
+# An opt-in table (convert(..., pin_table=NANGATE45_PINS)) for the cells of
+# Nangate45-style libraries that the table above lacks or names otherwise
+# (its AND2 has pins A, B, Y).  Inputs number 1-4 in pin order, a MUX's
+# select is pin 5, the output is pin 0; BUF becomes a one-input AND, which
+# is a buffer.  Not in the reference: with it a dump converts without
+# pin-0 fallbacks.
+NANGATE45_PINS = dict(
+    {"AND%d" % n: dict({"A%d" % i: i for i in range(1, n + 1)}, ZN=0) for n in (2, 3, 4)},
+    **{"OR%d" % n: dict({"A%d" % i: i for i in range(1, n + 1)}, ZN=0) for n in (2, 3, 4)},
+    XOR2={"A": 1, "B": 2, "Z": 0},
+    XNOR2={"A": 1, "B": 2, "ZN": 0},
+    BUF={"A": 1, "Z": 0},
+    MUX2={"A": 1, "B": 2, "S": 5, "Z": 0},
+)
+
 # Gate type by cell-type prefix, first match wins (fsim/parser.py:57-72,
 # 82-88); GateType numbering of fsim/base_ppg.hpp.
 TYPE_PREFIXES = [

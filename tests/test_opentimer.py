@@ -172,6 +172,30 @@ def test_high_fanout_net_whose_sinks_were_all_taken():
     assert len(w[(1, 0)]) == n and all(pin == 1 for _, pin in w[(1, 0)])
 
 
+def test_nangate45_table_converts_without_fallbacks():
+    """With the opt-in table, a dump over AND/OR 2-4, XOR2, XNOR2, BUF, MUX2
+    and the reference's INV/NAND/NOR/AOI/OAI/DFF cells converts in strict
+    mode; the netlist loads, MUX selects land on pin 5 and the oracle runs
+    it."""
+    table = dict(opentimer.PIN_TABLE)
+    table.update(opentimer.NANGATE45_PINS)
+    for k in ("AND2X1", "INVX1", "NAND3X1"):  # the reference's X1-suffixed variants
+        table.pop(k)
+    d = gen.opentimer_dump(1500, 40, seed=11, window=10, pins=table)  # acyclic: no input is cut
+    warnings = []
+    ckt = opentimer.convert(d, "loops", pin_table=opentimer.NANGATE45_PINS, strict=True,
+                            warnings=warnings)
+    assert all("unknown gate name" in w and w.startswith("BUF") for w in warnings)
+    types = [int(t) for t in ckt.strip().split("\n")[-1].split()]
+    assert 7 in types and 3 in types and 6 in types and 2 in types
+    assert any(pin == 5 for _, sinks in wires_of(ckt) for _, pin in sinks)
+    s = Simulator(-1)
+    s.load_circuit(ckt)
+    n_pi = int(ckt.split("\n")[0])
+    o = Oracle(ckt, gen.faults(ckt, "outputs"), gen.patterns(n_pi, 300, seed=1))
+    assert len(o.simulate()) > 0
+
+
 def test_tables_and_errors():
     assert opentimer.gate_type("NAND2_X1") == 4 and opentimer.gate_type("XNOR2_X1") == 6
     assert opentimer.gate_type("AOI22_X2") == 4 and opentimer.gate_type("OAI21_X1") == 5
