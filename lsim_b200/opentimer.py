@@ -36,6 +36,9 @@ Where it differs, on purpose:
   * the reference removes the edges to every sink whose name merely starts
     with the taken element's name (u1 also matches u12:A); here the names
     must be equal;
+  * compat=True (--compat) undoes the first two: sinks in Python sets and
+    removal by prefix, so that the output is byte-identical to the
+    reference's under the same interpreter and PYTHONHASHSEED;
   * mode "loops" (not in the reference) cuts only edges that close a
     cycle: a topological walk from the PIs that, whenever every element left
     waits on a cycle, cuts the unprocessed inputs of the waiting element
@@ -159,6 +162,30 @@ def _walk_reference(sinks, pis, po_set, mode, warnings):
         todo.extend(out for out in outs if out not in taken)
 
 
+def _walk_compat(sinks, pis, po_set, mode, warnings):
+    """The reference's walk step for step on its own data structure (sinks
+    in Python sets, removal by name prefix, one rebuild per taken sink
+    element), so that set iteration orders, and with them the output, are
+    the reference's under the same interpreter and hash seed."""
+    todo = deque(pis)
+    taken = set()
+    while todo:
+        cur = todo.popleft() if mode == "bfs" else todo.pop()
+        if cur in taken:
+            continue
+        taken.add(cur)
+        key = next((cur + s for s in OUTPUT_SUFFIXES if cur + s in sinks), None)
+        if key is None:
+            if cur not in po_set and warnings is not None:
+                warnings.append("no connection found for %s" % cur)
+            continue
+        for out in [x.split(":")[0] for x in sinks[key]]:
+            if out in taken:
+                sinks[key] = {x for x in sinks[key] if not x.startswith(out)}
+            else:
+                todo.append(out)
+
+
 def _walk_loops(sinks, listing):
     """Cuts the fewest inputs it can to make the netlist acyclic: a
     topological walk (Kahn) from the elements without inputs, PIs first;
@@ -206,15 +233,20 @@ def _walk_loops(sinks, listing):
         sinks[key] = [x for i, x in enumerate(sinks[key]) if (key, i) not in cut]
 
 
-def convert(text, mode="bfs", pin_table=None, strict=False, warnings=None):
+def convert(text, mode="bfs", pin_table=None, strict=False, warnings=None, compat=False):
     """.ckt text of an OpenTimer dump.
     mode: "bfs" or "dfs" (the reference's loop breaking) or "loops".
     pin_table: extra cells (name -> {pin: number}) beside PIN_TABLE.
     strict: an edge to a pin missing from the tables raises ValueError
     instead of being written as pin 0.
-    warnings: a list that receives the notes the reference prints."""
+    warnings: a list that receives the notes the reference prints.
+    compat: keep sinks in Python sets and remove them by name prefix, as
+    the reference does: the output is then byte-identical to fsim/parser.py
+    run by the same interpreter under the same PYTHONHASHSEED (bfs and dfs)."""
     if mode not in MODES:
         raise ValueError("unknown mode %r (bfs, dfs or loops)" % (mode,))
+    if compat and mode == "loops":
+        raise ValueError("compat reproduces the reference's bfs and dfs modes only")
     pins_of = dict(PIN_TABLE)
     if pin_table:
         pins_of.update(pin_table)
@@ -234,11 +266,15 @@ def convert(text, mode="bfs", pin_table=None, strict=False, warnings=None):
     for src, dst in edges:
         if src.split(":")[0] == dst.split(":")[0]:
             continue  # an arc inside one cell
-        if (src, dst) not in seen:
+        if compat:
+            sinks.setdefault(src, set()).add(dst)
+        elif (src, dst) not in seen:
             seen.add((src, dst))
             sinks.setdefault(src, []).append(dst)
 
-    if mode == "loops":
+    if compat:
+        _walk_compat(sinks, pis, po_set, mode, warnings)
+    elif mode == "loops":
         _walk_loops(sinks, pis + [c[0] for c in cells] + pos)
     else:
         _walk_reference(sinks, pis, po_set, mode, warnings)
@@ -270,13 +306,14 @@ def convert(text, mode="bfs", pin_table=None, strict=False, warnings=None):
     return "\n".join(out) + "\n"
 
 
-def convert_file(src, dst, mode="bfs", strict=False):
+def convert_file(src, dst, mode="bfs", strict=False, compat=False):
     """fsim/parser.py's command line (python parser.py <in> <out> <mode>):
-    python -m lsim_b200.opentimer <in> <out> <mode>.  Returns the warnings."""
+    python -m lsim_b200.opentimer <in> <out> <mode> [--compat].  Returns the
+    warnings."""
     with open(src) as f:
         text = f.read()
     warnings = []
-    ckt = convert(text, mode, strict=strict, warnings=warnings)
+    ckt = convert(text, mode, strict=strict, warnings=warnings, compat=compat)
     with open(dst, "w") as f:
         f.write(ckt)
     return warnings
@@ -284,13 +321,16 @@ def convert_file(src, dst, mode="bfs", strict=False):
 
 def main(argv=None):
     import sys
-    argv = sys.argv[1:] if argv is None else argv
+    argv = list(sys.argv[1:] if argv is None else argv)
+    compat = "--compat" in argv
+    if compat:
+        argv.remove("--compat")
     if len(argv) != 3:
-        print("usage: python -m lsim_b200.opentimer <dump> <out.ckt> <bfs|dfs|loops>",
+        print("usage: python -m lsim_b200.opentimer <dump> <out.ckt> <bfs|dfs|loops> [--compat]",
               file=sys.stderr)
         return 2
     try:
-        for w in convert_file(argv[0], argv[1], argv[2]):
+        for w in convert_file(argv[0], argv[1], argv[2], compat=compat):
             print("Warning:", w)
     except (OSError, ValueError) as e:
         print("error:", e, file=sys.stderr)

@@ -17,6 +17,12 @@ order.  The cases where that holds by construction:
   * a small dump with cell types missing from the tables (pin 0 and the AND
     default, with the reference's warnings).
 
+``compat`` records hold dumps whose output does depend on the hash seed
+(fanout and equal-depth edges), with the reference's exact output under
+PYTHONHASHSEED 0, 5 and 11 and the interpreter version that produced it:
+the converter's compat mode must reproduce those bytes under the same seed
+and interpreter.
+
 Run from the repository root with the reference checked out at
 ``/root/reference``:  ``python tests/golden/make_opentimer.py``
 """
@@ -117,6 +123,16 @@ def cases():
     return out
 
 
+COMPAT_SEEDS = (0, 5, 11)
+
+
+def compat_cases():
+    out = [("fanout_%d" % s, gen.opentimer_dump(40 + 10 * s, 6 + s, seed=50 + s, loops=2 + s), ("bfs", "dfs"))
+           for s in range(4)]
+    out.append(("prefix_names", PREFIX_DUMP, ("bfs", "dfs")))
+    return out
+
+
 def canonical(ckt):
     """(header, wire lines with sorted sinks, type line) of .ckt text."""
     ls = ckt.strip("\n").split("\n")
@@ -141,7 +157,7 @@ def run_reference(dump, mode, seed, tmp):
 
 
 def main():
-    recs = []
+    recs, dumps = [], {}
     with tempfile.TemporaryDirectory(dir=HERE) as tmp:
         for name, dump, modes in cases():
             for mode in modes:
@@ -151,12 +167,19 @@ def main():
                     raise SystemExit("%s/%s: the reference's output depends on the hash seed" %
                                      (name, mode))
                 warnings = [ln for ln in outs[0][1].split("\n") if ln.startswith("Warning")]
-                recs.append(dict(name=name, mode=mode, dump=dump, ckt=outs[0][0],
-                                 n_warnings=len(warnings)))
+                dumps[name] = dump
+                recs.append(dict(name=name, mode=mode, ckt=outs[0][0], n_warnings=len(warnings)))
+        compat = []
+        for name, dump, modes in compat_cases():
+            for mode in modes:
+                outs = {str(sd): run_reference(dump, mode, sd, tmp)[0] for sd in COMPAT_SEEDS}
+                dumps[name] = dump
+                compat.append(dict(name=name, mode=mode, ckt=outs))
     path = os.path.join(HERE, "opentimer_ref.json")
     with open(path, "w") as f:
         json.dump(dict(source="fsim/parser.py run under PYTHONHASHSEED in %s" % (SEEDS,),
-                       cases=recs), f, indent=0)
+                       dumps=dumps, cases=recs, python="%d.%d" % sys.version_info[:2], compat=compat),
+                  f, indent=0)
         f.write("\n")
     print("wrote %s: %d cases" % (path, len(recs)))
 

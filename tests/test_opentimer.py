@@ -4,19 +4,24 @@ breaking, and the converted netlists through the reader, the oracle and
 (marked gpu) the GPU path."""
 import json
 import os
+import subprocess
+import sys
 from collections import deque
 
 import numpy as np
 import pytest
 
 from lsim_b200 import Simulator, gen, opentimer
-from tests.conftest import GOLDEN
+from tests.conftest import GOLDEN, ROOT
 from tests.oracle_lib import Oracle, Reference, ref_available
 
 needs_ref = pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built here")
 
 with open(os.path.join(GOLDEN, "opentimer_ref.json")) as _f:
-    REF = json.load(_f)["cases"]
+    _FIX = json.load(_f)
+DUMPS_REF = _FIX["dumps"]
+REF = [dict(c, dump=DUMPS_REF[c["name"]]) for c in _FIX["cases"]]
+COMPAT = [dict(c, dump=DUMPS_REF[c["name"]]) for c in _FIX["compat"]]
 
 
 def canonical(ckt):
@@ -70,6 +75,23 @@ def test_matches_the_reference_converter(case):
     assert len(warnings) == case["n_warnings"]
     if all(len(s) <= 1 for _, s in wires_of(got)):
         assert got == case["ckt"]  # nothing for a set to reorder: byte-identical
+
+
+@pytest.mark.skipif("%d.%d" % sys.version_info[:2] != _FIX["python"],
+                    reason="Python set order is specific to the interpreter version")
+@pytest.mark.parametrize("case", COMPAT, ids=lambda c: "%s-%s" % (c["name"], c["mode"]))
+def test_compat_mode_is_byte_identical_under_the_same_hash_seed(case, tmp_path):
+    """Dumps whose reference output changes with the hash seed: in compat
+    mode, run under the same PYTHONHASHSEED, the converter writes the
+    reference's bytes (recorded for seeds 0, 5 and 11)."""
+    src = tmp_path / "dump.txt"
+    src.write_text(case["dump"])
+    for seed, want in case["ckt"].items():
+        dst = tmp_path / ("out%s.ckt" % seed)
+        subprocess.run([sys.executable, "-m", "lsim_b200.opentimer", str(src), str(dst), case["mode"],
+                        "--compat"], env=dict(os.environ, PYTHONHASHSEED=seed), cwd=ROOT,
+                       check=True, capture_output=True)
+        assert dst.read_text() == want, seed
 
 
 def test_prefix_names_differ_only_where_documented():
