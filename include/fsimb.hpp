@@ -13,7 +13,8 @@
  *                           the same run; num_threads is accepted and unused)
  *   g_pi/g_gate/g_po_results(), found_fault_to_pattern(),
  *   gate_idx_to_tpg_order_idx(), num_gates_per_level(), num_PIs/... ,
- *   visualization_graph(path)
+ *   pi(i)/gate(i)/po(i)/gates() with idx()/level()/output_value(),
+ *   gateTypeToString(type), visualization_graph(path)
  * Beyond the reference: results() gives per fault the detected flag, first
  * detecting pattern and detection count.  Errors other than a missing file
  * throw fsimb::Error (a std::runtime_error) carrying the status code.
@@ -42,9 +43,30 @@ class Error : public std::runtime_error {
   int code_;
 };
 
+/* Gate type numbering of fsim/base_ppg.hpp:19-32 (PI and PO follow CLKBUF). */
+enum class GateType : int { INV = 0, AND, OR, XOR, NAND, NOR, XNOR, MUX, CLKBUF, PI, PO };
+
 class Simulator {
  public:
   enum class Mode { SEQUENTIAL = 0, PARALLEL_TF, PARALLEL_OMP, CUDA_B200 };
+
+  /* An element as ElementBase's public interface shows it
+   * (fsim/base_ppg.hpp:47-50): idx() is the topological index, level() the
+   * level; output_value() is the element's good-machine word of the last
+   * round after run() and 0 before (the reference leaves there the word of
+   * its last faulty-machine simulation). */
+  class Element {
+   public:
+    size_t idx() const { return idx_; }
+    size_t level() const { return level_; }
+    size_t output_value() const { return value_; }
+    GateType type() const { return type_; }
+
+   private:
+    friend class Simulator;
+    size_t idx_ = 0, level_ = 0, value_ = 0;
+    GateType type_ = GateType::INV;
+  };
 
   /* device: CUDA device for run(); -1 for a host-only object that reads and
    * answers the accessors but cannot run. */
@@ -94,6 +116,23 @@ class Simulator {
   const std::vector<size_t>& gate_idx_to_tpg_order_idx() const { return tpg_; }
   const std::vector<size_t>& num_gates_per_level() const { return per_level_; }
 
+  /* fsim/simulation.hpp:58-63: elements by position among the PIs, gates, POs. */
+  Element pi(size_t i) const { return element(i); }
+  Element gate(size_t i) const { return element((size_t)info_.num_pis + i); }
+  Element po(size_t i) const { return element((size_t)(info_.num_pis + info_.num_gates) + i); }
+  std::vector<Element> gates() const {
+    std::vector<Element> g;
+    for (size_t i = 0; i < (size_t)info_.num_gates; ++i) g.push_back(gate(i));
+    return g;
+  }
+  /* fsim/simulation.cpp:1127-1155 */
+  std::string gateTypeToString(GateType type) const {
+    static const char* const names[] = {"INV", "AND", "OR",     "XOR", "NAND", "NOR",
+                                        "XNOR", "MUX", "CLKBUF", "PI",  "PO"};
+    const int t = (int)type;
+    return t >= 0 && t <= 10 ? names[t] : "UNKNOWN";
+  }
+
   void visualization_graph(const std::string& output_file) {
     char* text = nullptr;
     size_t len = 0;
@@ -118,7 +157,8 @@ class Simulator {
  private:
   fsimb_handle* h_ = nullptr;
   fsimb_info info_{};
-  std::vector<size_t> tpg_, per_level_, g_pi_, g_gate_, g_po_, found_;
+  std::vector<size_t> tpg_, per_level_, levels_, g_pi_, g_gate_, g_po_, found_;
+  std::vector<uint8_t> types_;
   std::vector<fsimb_fault_result> results_;
 
   static std::string slurp(std::istream& s) {
@@ -140,11 +180,32 @@ class Simulator {
     check(fsimb_gates_per_level(h_, l.data(), l.size()));
     tpg_ = to_size(t);
     per_level_ = to_size(l);
+    std::vector<uint64_t> lv(info_.num_elements);
+    check(fsimb_levels(h_, lv.data(), lv.size()));
+    levels_ = to_size(lv);
+    types_.assign(info_.num_elements, 0);
+    check(fsimb_types(h_, types_.data(), types_.size()));
     g_pi_.clear();
     g_gate_.clear();
     g_po_.clear();
     found_.clear();
     results_.clear();
+  }
+
+  Element element(size_t t) const {
+    if (t >= levels_.size()) throw std::out_of_range("element index out of range");
+    Element e;
+    e.idx_ = t;
+    e.level_ = levels_[t];
+    e.type_ = (GateType)types_[t];
+    const size_t np = g_pi_.size(), ng = g_gate_.size();
+    if (t < np)
+      e.value_ = g_pi_[t];
+    else if (t < np + ng)
+      e.value_ = g_gate_[t - np];
+    else if (t - np - ng < g_po_.size())
+      e.value_ = g_po_[t - np - ng];
+    return e;
   }
 
   void load_results() {

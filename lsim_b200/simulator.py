@@ -31,6 +31,36 @@ def _u64p(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
 
 
+# GateType names of fsim/base_ppg.hpp:19-32, as gateTypeToString gives them.
+GATE_TYPE_NAMES = ["INV", "AND", "OR", "XOR", "NAND", "NOR", "XNOR", "MUX", "CLKBUF", "PI", "PO"]
+
+
+class Element:
+    """An element as ElementBase's public interface shows it
+    (fsim/base_ppg.hpp:47-50): idx() is the topological index, level() the
+    level; output_value() is the element's good-machine word of the last
+    round after run() and 0 before (the reference leaves there the word of
+    its last faulty-machine simulation).  `type` is the GateType number."""
+
+    __slots__ = ("_idx", "_level", "type", "_value")
+
+    def __init__(self, idx, level, type_, value):
+        self._idx, self._level, self.type, self._value = idx, level, type_, value
+
+    def idx(self):
+        return self._idx
+
+    def level(self):
+        return self._level
+
+    def output_value(self):
+        return self._value
+
+    def __repr__(self):
+        return "Element(idx=%d, level=%d, type=%s)" % (self._idx, self._level,
+                                                       Simulator.gateTypeToString(self.type))
+
+
 class Simulator:
     class Mode(enum.IntEnum):
         SEQUENTIAL = 0
@@ -187,6 +217,38 @@ class Simulator:
     def num_rounds(self):
         return self.info().num_rounds
 
+    def pi(self, i):
+        """fsim/simulation.hpp:58-63: the i-th PI, gate or PO as an Element."""
+        return self._element(int(i), 0, self.num_PIs())
+
+    def gate(self, i):
+        return self._element(int(i), self.num_PIs(), self.num_gates())
+
+    def po(self, i):
+        return self._element(int(i), self.num_PIs() + self.num_gates(), self.num_POs())
+
+    def gates(self):
+        n_pi, n_g = self.num_PIs(), self.num_gates()
+        lv, ty, val = self.levels(), self.types(), self._values()
+        return [Element(t, int(lv[t]), int(ty[t]), int(val[t])) for t in range(n_pi, n_pi + n_g)]
+
+    @staticmethod
+    def gateTypeToString(t):
+        """fsim/simulation.cpp:1127-1155."""
+        t = int(t)
+        return GATE_TYPE_NAMES[t] if 0 <= t < len(GATE_TYPE_NAMES) else "UNKNOWN"
+
+    def _values(self):
+        if self._ran and self.info().num_rounds:
+            return self.good_values()
+        return np.zeros(self.info().num_elements, dtype=np.uint64)
+
+    def _element(self, i, first, count):
+        if not 0 <= i < count:
+            raise IndexError("element index out of range")
+        t = first + i
+        return Element(t, int(self.levels()[t]), int(self.types()[t]), int(self._values()[t]))
+
     def gate_idx_to_tpg_order_idx(self):
         n = self.info().num_elements
         out = np.zeros(n, dtype=np.uint64)
@@ -250,4 +312,4 @@ class Simulator:
         return out.reshape(i.num_rounds, i.num_pis)
 
 
-__all__ = ["Simulator", "FsimbError", "RESULT_DTYPE"]
+__all__ = ["Simulator", "Element", "GATE_TYPE_NAMES", "FsimbError", "RESULT_DTYPE"]

@@ -7,6 +7,7 @@ import subprocess
 import pytest
 
 from lsim_b200 import build
+from tests.oracle_lib import Oracle
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -50,6 +51,12 @@ def test_shim_reads_like_the_reference(shim, basics, tmp_path, t):
     assert d["tpg"] == a["tpg_ans"][t]
     assert d["per_level"] == a["num_gate_per_lvl_ans"][t]
     assert (tmp_path / "g.dot").read_text().startswith("digraph G {")
+    n = sum(a["num_vars_ans"][t][:3])
+    assert d["elem_idx"] == list(range(n))
+    o = Oracle(c["ckt"], c["flst"], c["ptn"])
+    assert d["elem_level"] == [int(x) for x in o.levels()]
+    assert d["elem_type"] == [int(x) for x in o.types()]
+    assert d["type_names_ok"] == [1]
 
 
 def test_shim_missing_file_message(shim, tmp_path):
@@ -70,5 +77,6 @@ def test_shim_runs_like_the_reference(shim, basics, tmp_path, t):
     d = _parse(r.stdout)
     assert d["g_pi"] == a["pi_ans"][t]
     assert d["g_gate"] == a["gate_ans"][t]
+    assert d["gate_output_values"] == d["g_gate"]
     assert d["g_po"] == a["po_ans"][t]
     assert d["found"] == a["found_flst_2_ptn_ans"][t]

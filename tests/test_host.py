@@ -281,3 +281,26 @@ def test_loader_selection_on_a_host_handle():
         assert li["ms_total"] >= 0
     with pytest.raises(KeyError):
         s.set_loader("gpu")
+
+
+def test_element_accessors_like_the_reference():
+    """pi(i) / gate(i) / po(i) / gates() (fsim/simulation.hpp:58-63) with
+    ElementBase's idx() / level() / output_value(), and gateTypeToString."""
+    from lsim_b200 import Simulator as S
+    w = gen.generate(n_gates=120, n_pi=9, n_po=7, n_levels=8, n_patterns=100, seed=4,
+                     type_mask=gen.ALL_TYPES)
+    s = S(-1)
+    s.read_text(w["ckt"], w["flst"], w["ptn"])
+    o = Oracle(w["ckt"], w["flst"], w["ptn"])
+    lv, ty = o.levels(), o.types()
+    elems = [s.pi(i) for i in range(9)] + s.gates() + [s.po(i) for i in range(7)]
+    assert [e.idx() for e in elems] == list(range(9 + 120 + 7))
+    assert [e.level() for e in elems] == [int(x) for x in lv]
+    assert [e.type for e in elems] == [int(x) for x in ty]
+    assert all(e.output_value() == 0 for e in elems)  # before run()
+    assert s.gate(5).idx() == 14 and s.po(0).idx() == 129
+    assert [S.gateTypeToString(t) for t in range(12)] == [
+        "INV", "AND", "OR", "XOR", "NAND", "NOR", "XNOR", "MUX", "CLKBUF", "PI", "PO", "UNKNOWN"]
+    with pytest.raises(IndexError):
+        s.pi(9)
+    assert s.num_pos() == 7
