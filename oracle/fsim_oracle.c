@@ -405,16 +405,18 @@ static void run_naive(const job_t* j) {
   free(b);
 }
 
-/* Same results, propagating only through the fault's fanout cone in
- * topological order (min-heap of pending elements). */
+/* Same results, propagating only through the fault's fanout cone: pending
+ * elements are bits of a bitmap scanned upward from the fault site.  Every
+ * consumer has a larger topological index than its fanins, so one forward
+ * scan visits the pending elements in topological order. */
 static void run_event(const job_t* j) {
   const or_netlist* nl = j->nl;
   const uint64_t N = nl->N;
+  const uint64_t NW = (N + 63) / 64;
   uint64_t* g = malloc(N * 8);
   uint64_t* b = malloc(N * 8);
   uint32_t* stamp = calloc(N, sizeof(uint32_t)); /* b[i] valid for this fault */
-  uint32_t* queued = calloc(N, sizeof(uint32_t));
-  uint64_t* heap = malloc((N + 1) * 8);
+  uint64_t* pend = calloc(NW, sizeof(uint64_t));
   uint32_t epoch = 0;
   const uint64_t W = (j->P + 63) / 64;
   for (uint64_t rd = j->rd0; rd < j->rd1; rd++) {
@@ -424,52 +426,38 @@ static void run_event(const job_t* j) {
       const or_fault* f = &j->faults[fi];
       const uint64_t sv = f->value ? ~0ull : 0ull;
       epoch++;
-      uint64_t hn = 0;
-      heap[hn++] = f->site;
-      queued[f->site] = epoch;
+      pend[f->site >> 6] |= 1ull << (f->site & 63);
+      uint64_t npend = 1;
       uint64_t diff = 0;
-      while (hn) {
-        /* pop min */
-        uint64_t i = heap[0];
-        heap[0] = heap[--hn];
-        for (uint64_t c = 0;;) {
-          uint64_t l = 2 * c + 1, r = l + 1, m = c;
-          if (l < hn && heap[l] < heap[m]) m = l;
-          if (r < hn && heap[r] < heap[m]) m = r;
-          if (m == c) break;
-          uint64_t tmp = heap[c];
-          heap[c] = heap[m];
-          heap[m] = tmp;
-          c = m;
-        }
-        uint64_t v;
-        if (i == f->site && f->pin == 0) {
-          v = sv;
-        } else {
-          uint64_t in[4];
-          uint64_t n = nl->fi_off[i + 1] - nl->fi_off[i];
-          for (uint64_t k = 0; k < n; k++) {
-            uint64_t d = nl->fi_idx[nl->fi_off[i] + k];
-            in[k] = (stamp[d] == epoch) ? b[d] : g[d];
+      for (uint64_t w = f->site >> 6; w < NW && npend; w++) {
+        while (pend[w]) {
+          const uint64_t i = w * 64 + (uint64_t)__builtin_ctzll(pend[w]);
+          pend[w] &= pend[w] - 1;
+          npend--;
+          uint64_t v;
+          if (i == f->site && f->pin == 0) {
+            v = sv;
+          } else {
+            uint64_t in[4];
+            uint64_t n = nl->fi_off[i + 1] - nl->fi_off[i];
+            for (uint64_t k = 0; k < n; k++) {
+              uint64_t d = nl->fi_idx[nl->fi_off[i] + k];
+              in[k] = (stamp[d] == epoch) ? b[d] : g[d];
+            }
+            if (i == f->site) in[f->pin - 1] = sv;
+            v = eval_gate(nl->type[i], in, n);
           }
-          if (i == f->site) in[f->pin - 1] = sv;
-          v = eval_gate(nl->type[i], in, n);
-        }
-        if (v == g[i]) continue; /* no difference leaves this element */
-        b[i] = v;
-        stamp[i] = epoch;
-        if (i >= nl->po_begin) diff |= (g[i] ^ v) & mask;
-        for (uint64_t k = nl->fo_off[i]; k < nl->fo_off[i + 1]; k++) {
-          uint64_t c = nl->fo_idx[k];
-          if (queued[c] == epoch) continue;
-          queued[c] = epoch;
-          uint64_t pos = hn++;
-          heap[pos] = c;
-          while (pos && heap[(pos - 1) / 2] > heap[pos]) {
-            uint64_t tmp = heap[pos];
-            heap[pos] = heap[(pos - 1) / 2];
-            heap[(pos - 1) / 2] = tmp;
-            pos = (pos - 1) / 2;
+          if (v == g[i]) continue; /* no difference leaves this element */
+          b[i] = v;
+          stamp[i] = epoch;
+          if (i >= nl->po_begin) diff |= (g[i] ^ v) & mask;
+          for (uint64_t k = nl->fo_off[i]; k < nl->fo_off[i + 1]; k++) {
+            const uint64_t c = nl->fo_idx[k];
+            const uint64_t m = 1ull << (c & 63);
+            if (!(pend[c >> 6] & m)) {
+              pend[c >> 6] |= m;
+              npend++;
+            }
           }
         }
       }
@@ -479,14 +467,157 @@ static void run_event(const job_t* j) {
   free(g);
   free(b);
   free(stamp);
-  free(queued);
-  free(heap);
+  free(pend);
+}
+
+/* Gate functions over nr words at once (the same functions as eval_gate,
+ * word by word). */
+static void eval_vec(uint8_t ty, const uint64_t* const* in, uint64_t n, uint64_t* v, uint64_t nr) {
+  uint64_t r, k;
+  switch (ty) {
+    case T_INV:
+      for (r = 0; r < nr; r++) v[r] = ~in[0][r];
+      return;
+    case T_AND:
+    case T_NAND:
+      for (r = 0; r < nr; r++) {
+        uint64_t x = in[0][r];
+        for (k = 1; k < n; k++) x &= in[k][r];
+        v[r] = ty == T_NAND ? ~x : x;
+      }
+      return;
+    case T_OR:
+    case T_NOR:
+      for (r = 0; r < nr; r++) {
+        uint64_t x = in[0][r];
+        for (k = 1; k < n; k++) x |= in[k][r];
+        v[r] = ty == T_NOR ? ~x : x;
+      }
+      return;
+    case T_XOR:
+    case T_XNOR:
+      for (r = 0; r < nr; r++) {
+        uint64_t x = in[0][r];
+        for (k = 1; k < n; k++) x ^= in[k][r];
+        v[r] = ty == T_XNOR ? ~x : x;
+      }
+      return;
+    case T_MUX:
+      for (r = 0; r < nr; r++) v[r] = (in[2][r] & in[1][r]) | (in[0][r] & (uint64_t)(!in[2][r]));
+      return;
+    default: /* CLKBUF, PO */
+      for (r = 0; r < nr; r++) v[r] = in[0][r];
+      return;
+  }
+}
+
+/* The event-driven propagation of run_event for a chunk of up to R rounds
+ * at once: an element is evaluated for every round of the chunk when any
+ * of its fanins differs in any round, and the per-round PO differences are
+ * folded into the results one round at a time.  Same results as modes 0
+ * and 1; the chunk turns one random access per element into R words. */
+static void run_event_chunked(const job_t* j) {
+  const or_netlist* nl = j->nl;
+  const uint64_t N = nl->N;
+  const uint64_t NW = (N + 63) / 64;
+  uint64_t R = (64ull << 20) / (N * 8 + 1); /* about 64 MB of faulty words per thread */
+  if (R > 64) R = 64;
+  if (R < 4) R = 4;
+  uint64_t* g = malloc(N * R * 8);
+  uint64_t* b = malloc(N * R * 8);
+  uint32_t* stamp = calloc(N, sizeof(uint32_t));
+  uint64_t* pend = calloc(NW, sizeof(uint64_t));
+  uint64_t* v = malloc(R * 8);
+  uint64_t* diff = malloc(R * 8);
+  uint64_t* mask = malloc(R * 8);
+  uint64_t* bitsv = malloc(R * 8);
+  uint64_t* svv = malloc(R * 8);
+  uint32_t epoch = 0;
+  const uint64_t W = (j->P + 63) / 64;
+  for (uint64_t c0 = j->rd0; c0 < j->rd1; c0 += R) {
+    const uint64_t nr = (j->rd1 - c0 < R) ? j->rd1 - c0 : R;
+    for (uint64_t r = 0; r < nr; r++) {
+      bitsv[r] = round_bits(j->P, c0 + r);
+      mask[r] = bits_mask(bitsv[r]);
+    }
+    /* good machine of the chunk, element-major [i][r] */
+    for (uint64_t i = 0; i < N; i++) {
+      uint64_t* gi = g + i * R;
+      if (nl->type[i] == T_PI) {
+        for (uint64_t r = 0; r < nr; r++) gi[r] = j->words[(c0 + r) * nl->n_pi + i];
+      } else {
+        const uint64_t* in[4];
+        uint64_t n = nl->fi_off[i + 1] - nl->fi_off[i];
+        for (uint64_t k = 0; k < n; k++) in[k] = g + nl->fi_idx[nl->fi_off[i] + k] * R;
+        eval_vec(nl->type[i], in, n, gi, nr);
+      }
+    }
+    for (uint64_t fi = j->f0; fi < j->f1; fi++) {
+      const or_fault* f = &j->faults[fi];
+      const uint64_t sv = f->value ? ~0ull : 0ull;
+      for (uint64_t r = 0; r < nr; r++) {
+        diff[r] = 0;
+        svv[r] = sv;
+      }
+      epoch++;
+      pend[f->site >> 6] |= 1ull << (f->site & 63);
+      uint64_t npend = 1;
+      for (uint64_t w = f->site >> 6; w < NW && npend; w++) {
+        while (pend[w]) {
+          const uint64_t i = w * 64 + (uint64_t)__builtin_ctzll(pend[w]);
+          pend[w] &= pend[w] - 1;
+          npend--;
+          const uint64_t* gi = g + i * R;
+          if (i == f->site && f->pin == 0) {
+            for (uint64_t r = 0; r < nr; r++) v[r] = sv;
+          } else {
+            const uint64_t* in[4];
+            uint64_t n = nl->fi_off[i + 1] - nl->fi_off[i];
+            for (uint64_t k = 0; k < n; k++) {
+              uint64_t d = nl->fi_idx[nl->fi_off[i] + k];
+              in[k] = ((stamp[d] == epoch) ? b : g) + d * R;
+            }
+            if (i == f->site) in[f->pin - 1] = svv;
+            eval_vec(nl->type[i], in, n, v, nr);
+          }
+          uint64_t changed = 0;
+          for (uint64_t r = 0; r < nr; r++) changed |= v[r] ^ gi[r];
+          if (!changed) continue; /* no difference leaves this element */
+          memcpy(b + i * R, v, nr * 8);
+          stamp[i] = epoch;
+          if (i >= nl->po_begin)
+            for (uint64_t r = 0; r < nr; r++) diff[r] |= (gi[r] ^ v[r]) & mask[r];
+          for (uint64_t k = nl->fo_off[i]; k < nl->fo_off[i + 1]; k++) {
+            const uint64_t c = nl->fo_idx[k];
+            const uint64_t m = 1ull << (c & 63);
+            if (!(pend[c >> 6] & m)) {
+              pend[c >> 6] |= m;
+              npend++;
+            }
+          }
+        }
+      }
+      for (uint64_t r = 0; r < nr; r++)
+        accumulate(&j->res[fi - j->base], diff[r], bitsv[r], c0 + r, W - 1);
+    }
+  }
+  free(g);
+  free(b);
+  free(stamp);
+  free(pend);
+  free(v);
+  free(diff);
+  free(mask);
+  free(bitsv);
+  free(svv);
 }
 
 static void* job_main(void* arg) {
   job_t* j = arg;
   if (j->mode == 0)
     run_naive(j);
+  else if (j->mode == 2)
+    run_event_chunked(j);
   else
     run_event(j);
   return NULL;

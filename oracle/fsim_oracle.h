@@ -77,7 +77,8 @@ void or_good_values(const or_netlist* nl, const uint64_t* words, uint64_t P, uin
 
 /* Fault simulation over rounds [rd0, rd1) for faults [f0, f1).  mode 0 is the
  * reference's full re-simulation per fault (fsim/simulation.cpp:186-228); mode
- * 1 propagates only through the fault's fanout cone (same results).
+ * 1 propagates only through the fault's fanout cone (same results); mode 2 is
+ * mode 1 over chunks of rounds at once (same results, for large circuits).
  * n_threads > 1 shards faults across POSIX threads.  Results are accumulated
  * into res[f - f0] (initialise with or_results_init). */
 void or_results_init(or_result* res, size_t n);
