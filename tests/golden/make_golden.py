@@ -13,8 +13,8 @@
    ref``), recording per-fault detected / first / count, the reference's
    found_fault_to_pattern table and the last round's good values.
 
-Run from the repository root with the reference checked out at
-``/root/reference``:  ``python tests/golden/make_golden.py``
+Run from the repository root with the reference tree named by
+LSIM_REFERENCE (default: a ``reference`` directory beside the repository):  ``python tests/golden/make_golden.py``
 """
 import ctypes
 import json
@@ -24,7 +24,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("LSIM_REFERENCE", "/root/reference")
+REF = os.environ.get("LSIM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def _strip_comments(src):

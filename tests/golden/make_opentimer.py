@@ -23,8 +23,8 @@ PYTHONHASHSEED 0, 5 and 11 and the interpreter version that produced it:
 the converter's compat mode must reproduce those bytes under the same seed
 and interpreter.
 
-Run from the repository root with the reference checked out at
-``/root/reference``:  ``python tests/golden/make_opentimer.py``
+Run from the repository root with the reference tree named by
+LSIM_REFERENCE (default: a ``reference`` directory beside the repository):  ``python tests/golden/make_opentimer.py``
 """
 import json
 import os
@@ -34,7 +34,7 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("LSIM_REFERENCE", "/root/reference")
+REF = os.environ.get("LSIM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 sys.path.insert(0, ROOT)
 
 from lsim_b200 import gen  # noqa: E402
