@@ -11,8 +11,8 @@ last-round flag comes from the rank that holds the last round.
 Fault sharding (strong scaling): rank r simulates its own part of the fault
 list over all patterns.  The parts keep every group of faults that share a
 sweep (one fanout-free region, fsimb_fault_costs) together and balance the
-groups' estimated costs; results combine with the same reductions, each
-fault being present on exactly one rank.
+groups' estimated costs; each fault lives on exactly one rank, so the merge
+gathers the parts (no reduction over the whole list).
 
 No data moves during simulation in either form.
 """
@@ -40,31 +40,41 @@ def local_patterns(words, n_patterns, n_pi, rank, world):
     return np.ascontiguousarray(w), P, r0 * 64
 
 
-def merge_results(res, first_pattern, holds_last_round, total_rounds, group=None, device="cpu"):
-    """All-reduce per-fault results of pattern shards into the full-block view.
+def merge_results(res, first_pattern, holds_last_round, total_rounds, group=None, device="cpu",
+                  dst=None):
+    """Reduce per-fault results of pattern shards into the full-block view.
 
     res: structured array with detected / first_pattern / count /
-    ref_last_round_flag (lsim_b200.RESULT_DTYPE).  Returns the merged array
-    (identical on every rank)."""
+    ref_last_round_flag (lsim_b200.RESULT_DTYPE).  Two reductions: count and
+    last-round flag together by SUM, first pattern by MIN.  dst=None: every
+    rank gets the merged array (all-reduce); dst=r: only rank r does (the
+    others get None), which halves the bytes each rank sends."""
     import torch
     import torch.distributed as dist
 
-    cnt = torch.from_numpy(res["count"].astype(np.int64)).to(device)
+    n = len(res)
+    sums = np.empty(2 * n, dtype=np.int64)
+    sums[:n] = res["count"].astype(np.int64)
+    sums[n:] = res["ref_last_round_flag"].astype(np.int64) * (1 if holds_last_round else 0)
     fp = res["first_pattern"].astype(np.int64)
     fp = np.where(fp < 0, INT64_MAX, fp + int(first_pattern))
+    st = torch.from_numpy(sums).to(device)
     first = torch.from_numpy(fp).to(device)
-    flag = torch.from_numpy(res["ref_last_round_flag"].astype(np.int64) *
-                            (1 if holds_last_round else 0)).to(device)
-    dist.all_reduce(cnt, op=dist.ReduceOp.SUM, group=group)
-    dist.all_reduce(first, op=dist.ReduceOp.MIN, group=group)
-    dist.all_reduce(flag, op=dist.ReduceOp.SUM, group=group)
-    out = np.zeros(len(res), dtype=res.dtype)
-    c = cnt.cpu().numpy()
+    if dst is None:
+        dist.all_reduce(st, op=dist.ReduceOp.SUM, group=group)
+        dist.all_reduce(first, op=dist.ReduceOp.MIN, group=group)
+    else:
+        dist.reduce(st, dst, op=dist.ReduceOp.SUM, group=group)
+        dist.reduce(first, dst, op=dist.ReduceOp.MIN, group=group)
+        if dist.get_rank() != dst:
+            return None
+    sm = st.cpu().numpy()
     f = first.cpu().numpy()
-    out["count"] = c.astype(np.uint64)
-    out["detected"] = (c > 0).astype(np.uint8)
+    out = np.zeros(n, dtype=res.dtype)
+    out["count"] = sm[:n].astype(np.uint64)
+    out["detected"] = (sm[:n] > 0).astype(np.uint8)
     out["first_pattern"] = np.where(f == INT64_MAX, -1, f)
-    out["ref_last_round_flag"] = flag.cpu().numpy().astype(np.uint8)
+    out["ref_last_round_flag"] = sm[n:].astype(np.uint8)
     out["ref_last_rd"] = max(0, total_rounds - 1)
     return out
 
@@ -128,16 +138,43 @@ def combine_fault_shards(parts, n_faults):
     return _assemble(cnt, first, flag, last_rd, dtype)
 
 
-def merge_fault_shards(res, idx, n_faults, total_rounds, group=None, device="cpu"):
-    """All-reduce the results of this rank's faults (indices idx) into the
-    results of the whole fault list (identical on every rank)."""
+def merge_fault_shards(res, idx, n_faults, total_rounds, group=None, device="cpu", dst=None):
+    """Gather the results of every rank's faults (this rank's: indices idx)
+    into the results of the whole fault list.  Each fault lives on one rank,
+    so only the parts move: every rank sends its own faults as rows of
+    (index | flag << 40, count, first pattern), padded to the longest part.
+    dst=None: every rank gets the merged array (all-gather); dst=r: only rank
+    r does (gather; the others get None)."""
     import torch
     import torch.distributed as dist
 
-    c, f, g = _fill(n_faults, idx, res)
-    cnt, first, flag = (torch.from_numpy(x).to(device) for x in (c, f, g))
-    dist.all_reduce(cnt, op=dist.ReduceOp.SUM, group=group)
-    dist.all_reduce(first, op=dist.ReduceOp.MIN, group=group)
-    dist.all_reduce(flag, op=dist.ReduceOp.SUM, group=group)
-    return _assemble(cnt.cpu().numpy(), first.cpu().numpy(), flag.cpu().numpy(),
-                     max(0, total_rounds - 1), res.dtype)
+    world = dist.get_world_size(group)
+    n_local = torch.tensor([len(idx)], dtype=torch.int64, device=device)
+    sizes = [torch.zeros_like(n_local) for _ in range(world)]
+    dist.all_gather(sizes, n_local, group=group)
+    width = max(int(x.item()) for x in sizes)
+    rows = np.zeros((width, 3), dtype=np.int64)
+    rows[:, 0] = -1
+    fp = res["first_pattern"].astype(np.int64)
+    rows[:len(idx), 0] = np.asarray(idx, dtype=np.int64) | (res["ref_last_round_flag"].astype(np.int64) << 40)
+    rows[:len(idx), 1] = res["count"].astype(np.int64)
+    rows[:len(idx), 2] = np.where(fp < 0, INT64_MAX, fp)
+    mine = torch.from_numpy(rows).to(device)
+    if dst is None:
+        parts = [torch.empty_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine, group=group)
+    else:
+        parts = [torch.empty_like(mine) for _ in range(world)] if dist.get_rank() == dst else None
+        dist.gather(mine, parts, dst=dst, group=group)
+        if dist.get_rank() != dst:
+            return None
+    allrows = torch.cat(parts).cpu().numpy()
+    allrows = allrows[allrows[:, 0] >= 0]
+    cnt = np.zeros(n_faults, dtype=np.int64)
+    first = np.full(n_faults, INT64_MAX, dtype=np.int64)
+    flag = np.zeros(n_faults, dtype=np.int64)
+    fi = allrows[:, 0] & ((1 << 40) - 1)
+    cnt[fi] = allrows[:, 1]
+    first[fi] = allrows[:, 2]
+    flag[fi] = allrows[:, 0] >> 40
+    return _assemble(cnt, first, flag, max(0, total_rounds - 1), res.dtype)

@@ -20,7 +20,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, w, q):
+def _worker(rank, world, port, w, q, dst=None):
     import torch.distributed as dist
     from tests.oracle_lib import Oracle
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -38,20 +38,20 @@ def _worker(rank, world, port, w, q):
         res["first_pattern"] = r["first"]
         res["ref_last_round_flag"] = r["ref_flag"]
         r0, r1 = shard.round_block(full.W, rank, world)
-        merged = shard.merge_results(res, first, r1 == full.W and r1 > r0, full.W)
-        q.put((rank, merged.tobytes()))
+        merged = shard.merge_results(res, first, r1 == full.W and r1 > r0, full.W, dst=dst)
+        q.put((rank, None if merged is None else merged.tobytes()))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("P", [64 * 40, 64 * 70 + 17])
-def test_pattern_shards_merge_to_full_block(P):
+@pytest.mark.parametrize("P,dst", [(64 * 40, None), (64 * 70 + 17, None), (64 * 70 + 17, 0)])
+def test_pattern_shards_merge_to_full_block(P, dst):
     w = gen.generate(n_gates=300, n_pi=12, n_po=10, n_levels=12, n_patterns=P, seed=77,
                      faults="collapsed")
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, w, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, w, q, dst)) for r in range(2)]
     for p in procs:
         p.start()
     outs = dict(q.get(timeout=120) for _ in range(2))
@@ -62,7 +62,9 @@ def test_pattern_shards_merge_to_full_block(P):
     ref = Oracle(w["ckt"], w["flst"], w["ptn"]).simulate()
     dt = np.dtype([("detected", np.uint8), ("ref_last_round_flag", np.uint8), ("pad", np.uint8, 6),
                    ("first_pattern", np.int64), ("count", np.uint64), ("ref_last_rd", np.uint64)])
-    for rank in range(2):
+    if dst is not None:
+        assert outs[1 - dst] is None
+    for rank in range(2) if dst is None else [dst]:
         m = np.frombuffer(outs[rank], dtype=dt)
         assert np.array_equal(m["count"], ref["count"])
         assert np.array_equal(m["first_pattern"], ref["first"])
@@ -71,7 +73,7 @@ def test_pattern_shards_merge_to_full_block(P):
         assert np.array_equal(m["ref_last_rd"], ref["ref_rd"])
 
 
-def _fault_worker(rank, world, port, w, q):
+def _fault_worker(rank, world, port, w, q, dst=None):
     import torch.distributed as dist
     from lsim_b200 import Simulator
     from tests.oracle_lib import Oracle
@@ -91,8 +93,8 @@ def _fault_worker(rank, world, port, w, q):
         res["first_pattern"] = r["first"]
         res["ref_last_round_flag"] = r["ref_flag"]
         res["ref_last_rd"] = r["ref_rd"]
-        merged = shard.merge_fault_shards(res, idx, len(site), h.info().num_rounds)
-        q.put((rank, merged.tobytes()))
+        merged = shard.merge_fault_shards(res, idx, len(site), h.info().num_rounds, dst=dst)
+        q.put((rank, None if merged is None else merged.tobytes()))
     finally:
         dist.destroy_process_group()
 
@@ -101,15 +103,17 @@ _DT = np.dtype([("detected", np.uint8), ("ref_last_round_flag", np.uint8), ("pad
                 ("first_pattern", np.int64), ("count", np.uint64), ("ref_last_rd", np.uint64)])
 
 
-def test_fault_shards_merge_to_full_list():
+@pytest.mark.parametrize("dst", [None, 0, 1])
+def test_fault_shards_merge_to_full_list(dst):
     """Each of 2 ranks simulates its part of the fault list over all patterns;
-    the merge equals one simulation of the whole list."""
+    the merge (gathered on every rank, or on rank dst only) equals one
+    simulation of the whole list."""
     w = gen.generate(n_gates=400, n_pi=12, n_po=10, n_levels=14, n_patterns=64 * 9 + 5, seed=78,
                      faults="pins", type_mask=gen.ALL_TYPES)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_fault_worker, args=(r, 2, port, w, q)) for r in range(2)]
+    procs = [ctx.Process(target=_fault_worker, args=(r, 2, port, w, q, dst)) for r in range(2)]
     for p in procs:
         p.start()
     outs = dict(q.get(timeout=120) for _ in range(2))
@@ -118,7 +122,9 @@ def test_fault_shards_merge_to_full_list():
         assert p.exitcode == 0
     from tests.oracle_lib import Oracle
     ref = Oracle(w["ckt"], w["flst"], w["ptn"]).simulate()
-    for rank in range(2):
+    if dst is not None:
+        assert outs[1 - dst] is None
+    for rank in range(2) if dst is None else [dst]:
         m = np.frombuffer(outs[rank], dtype=_DT)
         assert np.array_equal(m["count"], ref["count"])
         assert np.array_equal(m["first_pattern"], ref["first"])
