@@ -47,13 +47,17 @@ typedef struct {
   uint64_t ref_last_rd;        /* found_fault_to_pattern[2f+1] of the reference */
 } fsimb_fault_result;
 
-/* Run options.  Zero-initialise and set struct_size = sizeof(fsimb_opts). */
+/* Run options.  Zero-initialise and set struct_size = sizeof(fsimb_opts).
+ * A struct_size of the first seven fields (the layout before n_detect) is
+ * accepted too: the later fields then read as 0. */
 typedef struct {
   uint32_t struct_size;
   uint32_t drop;             /* 0: count mode (every pattern); 1: drop a fault
-                                after the 2048-pattern tile that first detects
-                                it (first_pattern exact, count covers that tile) */
-  uint32_t words_per_item;   /* sweep words per work item: 0 auto, or 1,2,4,8 */
+                                after the 2048-pattern tile in which its count
+                                reaches n_detect (first_pattern exact, count
+                                covers the patterns up to the end of that tile) */
+  uint32_t words_per_item;   /* sweep words per work item: 0 auto, or 1,2,4,8
+                                (1 or 2 for the wide-circuit sweep) */
   uint32_t block_threads;    /* sweep CTA size: 0 auto, or a multiple of 32 up to 1024 */
   uint32_t ctas_per_sm;      /* sweep CTAs sharing an SM: 0 auto, or 1..8; sizes the
                                 record buffer so that many fit */
@@ -61,6 +65,16 @@ typedef struct {
                                 fault list, time candidate sweep shapes on a strided sample
                                 of the first tile's sweeps and keep the fastest */
   void* stream;              /* cudaStream_t to run on; NULL: the handle's stream */
+  uint32_t n_detect;         /* with drop = 1: detections after which a fault is dropped
+                                (N-detect); 0 or 1: the first detection */
+  uint32_t sweep_variant;    /* 0 auto: live values in shared memory when they fit, else
+                                in global memory; 1 shared memory (FSIMB_ERR_LIMIT when
+                                they do not fit); 2 global memory */
+  uint32_t wait_test;        /* test hook, normally 0.  1: one sweep CTA waits on a barrier
+                                that no copy completes; the wait gives up after 20 ms and
+                                the run fails with FSIMB_ERR_CUDA, results discarded, the
+                                handle still usable.  Shared-memory sweep only. */
+  uint32_t pad;
 } fsimb_opts;
 
 /* Sizes of the loaded problem. */
@@ -94,7 +108,10 @@ typedef struct {
   uint64_t bank_access_groups;   /* sweep access groups (fanin loads and stores) per item */
   double ms_tune;            /* shape autotuning inside this run (0 when reused) */
   uint32_t ctas_per_sm;      /* sweep CTAs resident per SM */
-  uint32_t pad;
+  uint32_t sweep_variant;    /* 1: live values in shared memory; 2: in global memory */
+  uint64_t hbm_bytes_per_tile; /* compulsory DRAM bytes of one sweep launch: the tile's good
+                                  words, the schedule (gate records, live-in lists), the
+                                  sweep output rows */
 } fsimb_stats;
 
 /* Lifecycle.  fsimb_create fails with FSIMB_ERR_CUDA when `device` is not a
@@ -215,7 +232,11 @@ int fsimb_dot(const fsimb_handle* h, char** text, size_t* len);
  * before any stream capture.  All calls share the array and it keeps the last
  * call's contents; every value is written before it is read, so nothing needs
  * clearing, but calls whose kernels overlap on the GPU race on it.  Returns
- * after the kernels are enqueued on `stream` (NULL: the handle's stream). */
+ * after the kernels are enqueued on `stream` (NULL: the handle's stream).
+ * The kernels wait for the uploads of the handle's last fsimb_run, whatever
+ * stream it used; the caller orders what comes later on the handle (a run
+ * after new faults or a new circuit replaces the arrays these kernels read)
+ * after `stream`.  A device reset ends the handle and the looked-up address. */
 int fsimb_good_po_noalloc(fsimb_handle* h, const uint64_t* d_pattern_words, uint32_t n_words,
                           uint64_t* d_po_words, void* stream);
 

@@ -35,7 +35,9 @@ class Opts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("drop", ctypes.c_uint32),
                 ("words_per_item", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
                 ("ctas_per_sm", ctypes.c_uint32), ("tune", ctypes.c_uint32),
-                ("stream", ctypes.c_void_p)]
+                ("stream", ctypes.c_void_p), ("n_detect", ctypes.c_uint32),
+                ("sweep_variant", ctypes.c_uint32), ("wait_test", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
 
 
 class Info(ctypes.Structure):
@@ -56,7 +58,8 @@ class Stats(ctypes.Structure):
                 [("device_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
                  ("ms_compute", ctypes.c_double), ("bank_conflict_groups", ctypes.c_uint64),
                  ("bank_access_groups", ctypes.c_uint64), ("ms_tune", ctypes.c_double),
-                 ("ctas_per_sm", ctypes.c_uint32), ("pad", ctypes.c_uint32)])
+                 ("ctas_per_sm", ctypes.c_uint32), ("sweep_variant", ctypes.c_uint32),
+                 ("hbm_bytes_per_tile", ctypes.c_uint64)])
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -99,8 +99,8 @@ uint64_t batch_job_static_bytes(const BatchJob& j) {
     t(nl.fi_off.size() * 4);
     t(nl.fi_idx.size() * 4);
     t(nl.level.size() * 4);
-    t(p.level_off.size() * 4);
-    t(sc.recs.size() * sizeof(SweepRec));
+    t(sc.lvl.size() * sizeof(LevelDesc));
+    t(sc.blob.size() * 8);
     t(sc.li_off.size() * 4);
     t(sc.li.size() * 4);
   }
@@ -187,8 +187,8 @@ uint64_t BatchExec::upload_static(const std::vector<BatchJob>& jobs, cudaStream_
       c.fi_off = j.dev.fi_off;
       c.fi_idx = j.dev.fi_idx;
       c.level = j.dev.level;
-      c.level_off = j.dev.level_off;
-      c.recs = j.dev.recs;
+      c.lvl = j.dev.lvl;
+      c.blob = j.dev.blob;
       c.li_off = j.dev.li_off;
       c.li = j.dev.li;
     } else {
@@ -197,8 +197,8 @@ uint64_t BatchExec::upload_static(const std::vector<BatchJob>& jobs, cudaStream_
       c.fi_off = (const uint32_t*)put(nl.fi_off.data(), nl.fi_off.size() * 4);
       c.fi_idx = (const uint32_t*)put(nl.fi_idx.data(), nl.fi_idx.size() * 4);
       c.level = (const uint32_t*)put(nl.level.data(), nl.level.size() * 4);
-      c.level_off = (const uint32_t*)put(p.level_off.data(), p.level_off.size() * 4);
-      c.recs = (const uint4*)put(sc.recs.data(), sc.recs.size() * sizeof(SweepRec));
+      c.lvl = (const uint4*)put(sc.lvl.data(), sc.lvl.size() * sizeof(LevelDesc));
+      c.blob = (const uint4*)put(sc.blob.data(), sc.blob.size() * 8);
       c.li_off = (const uint32_t*)put(sc.li_off.data(), sc.li_off.size() * 4);
       c.li = (const uint32_t*)put(sc.li.data(), sc.li.size() * 4);
     }
@@ -337,9 +337,7 @@ void BatchExec::layout(const std::vector<BatchJob>& jobs, const std::vector<Clas
       items += ci_items;
       k.work += (double)jobs[i].plan->dense_sweep_gates * circs[i].tiles;
       max_live = std::max(max_live, jobs[i].sched->max_live);
-      const Plan& p = *jobs[i].plan;
-      for (uint32_t l = 1; l <= p.max_gate_level && l < p.n_levels; ++l)
-        widest = std::max(widest, p.level_off[l + 1] - p.level_off[l]);
+      widest = std::max(widest, jobs[i].sched->max_block16);
     }
     if (k.circ_ids.empty()) continue;
     k.n_items = items;
@@ -511,9 +509,9 @@ uint64_t BatchExec::enqueue_sweeps(cudaStream_t s, int only) {
       for (size_t j = j0; j < j1; ++j) {
         const BatchCirc& c = circs[k.circ_ids[j]];
         SweepCirc& d = params.c[j - j0];
-        d.recs = c.recs;
+        d.blob = c.blob;
         d.level = c.level;
-        d.level_off = c.level_off;
+        d.lvl = c.lvl;
         d.li_off = c.li_off;
         d.li = c.li;
         d.fi_off = c.fi_off;
@@ -530,6 +528,7 @@ uint64_t BatchExec::enqueue_sweeps(cudaStream_t s, int only) {
       }
       params.queue = d_ctl.as<unsigned long long>() + 1 + k.queue_base + j0;
       params.err = d_ctl.as<int>();
+      params.wait_ns = kWaitLimitNs;
       params.vals_bytes = k.vals_bytes;
       params.rec_buf = k.rec_buf;
       const int blocks = (int)std::min<unsigned long long>((unsigned long long)k.blocks, chunk_items);

@@ -32,8 +32,8 @@ struct BatchJob {
   uint64_t F = 0;
   int M = 4;
   int cls = 0;      // sweep class (index into the layout's shapes)
-  // resident: the circuit arrays (type, fi_off, fi_idx, level, level_off,
-  // recs, li_off, li) are dev's, already on the device.  good_resident:
+  // resident: the circuit arrays (type, fi_off, fi_idx, level, lvl, blob,
+  // li_off, li) are dev's, already on the device.  good_resident:
   // dev.good holds the job's good-machine tiles; no patterns are uploaded and
   // no good machine runs for it.
   bool resident = false;
@@ -54,7 +54,7 @@ struct SweepClass {
   unsigned long long n_items = 0;
   double work = 0;        // gate-words its sweeps evaluate (launch order)
   uint32_t max_live = 0;  // slots of the largest schedule in the class
-  uint32_t widest = 0;    // widest gate level in the class
+  uint32_t widest = 0;    // largest level block of gate records in the class, 16-byte units
   uint32_t vals_bytes = 0, rec_buf = 0;
   size_t smem = 0;
   int threads = 0, blocks = 0;

@@ -14,6 +14,7 @@
 #include <chrono>
 #include <functional>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <fstream>
 #include <mutex>
@@ -81,16 +82,18 @@ void default_sweep_shape(const Plan& plan, const std::function<const Schedule&(i
                          const std::function<int(int, int, size_t)>& occupancy,
                          std::vector<uint32_t> widths, uint32_t widest, size_t smem_optin,
                          size_t smem_per_sm, int& M, int& occ, int& threads) {
+  (void)widest;
   const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
   const size_t share2 = sweep_smem_share(smem_optin, smem_per_sm, 2);
   for (int m : {8, 4}) {
     // plan.max_live (no bank constraints) bounds every schedule's slots from below
-    if (sweep_vals_bytes(plan.max_live, m) + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
+    if (plan.max_live > kMaxSlots || sweep_vals_bytes(plan.max_live, m) + 64 * 32 > share2) continue;
     const Schedule& sc = sched_at(m);
     if (sc.max_live > kMaxSlots) continue;
     const uint32_t vals = sweep_vals_bytes(sc.max_live, m);
-    if (vals + std::min<uint32_t>(widest, 64) * 32 > share2) continue;
-    const size_t smem = vals + std::min<size_t>(widest, (share2 - vals) / 32) * 32;
+    const uint32_t blk = std::max<uint32_t>(sc.max_block16, 1);
+    if (vals + std::min<uint32_t>(blk, 64) * 32 > share2) continue;
+    const size_t smem = vals + std::min<size_t>(blk, (share2 - vals) / 32) * 32;
     int t = (int)std::min<uint32_t>(pick_sweep_threads(widths, m), sweep_max_threads(m));
     while (t > 64 && occupancy(m, t, smem) < 2) t -= 32;
     M = m;
@@ -170,11 +173,12 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
   for (const Cand& cd : cands) {
     const int M = cd.M, occ = cd.occ, T = cd.T;
     const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
-    if (sweep_vals_bytes(plan.max_live, M) > share1) continue;
+    if (plan.max_live > kMaxSlots || sweep_vals_bytes(plan.max_live, M) > share1) continue;
     const Schedule& sc = cached_schedule(M);
     if (sc.max_live > kMaxSlots || sweep_vals_bytes(sc.max_live, M) > share1) continue;
     if (cur_M != M) {
-      upload(d_recs, sc.recs, s);
+      upload(d_recs, sc.blob, s);
+      upload(d_lvl, sc.lvl, s);
       upload(d_li_off, sc.li_off, s);
       upload(d_li, sc.li, s);
       sched_uploaded = false;
@@ -183,8 +187,9 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     const uint32_t vals = sweep_vals_bytes(sc.max_live, M);
     const size_t share = sweep_smem_share(smem_optin, smem_per_sm, occ);
     if (vals > share) continue;
-    const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (share - vals) / 32);
-    if (occ > 1 && rec_buf < std::min<uint32_t>(widest, 64)) continue;
+    const uint32_t blk = std::max<uint32_t>(sc.max_block16, 1);
+    const uint32_t rec_buf = (uint32_t)std::min<size_t>(blk, (share - vals) / 32);
+    if (occ > 1 && rec_buf < std::min<uint32_t>(blk, 64)) continue;
     const size_t smem = std::max<size_t>(16, vals + (size_t)rec_buf * 32);
     if (T > (int)sweep_max_threads(M) || T * occ > 2048) continue;
     CK(sweep_set_smem(M, smem));
@@ -192,9 +197,9 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     CK(sweep_occupancy(M, T, smem, &got));
     if (got < occ) continue;  // the same as a shape with fewer CTAs per SM
     SweepArgs sa{};
-    sa.recs = d_recs.as<uint4>();
+    sa.blob = d_recs.as<uint4>();
+    sa.lvl = d_lvl.as<uint4>();
     sa.level = d_level.as<uint32_t>();
-    sa.level_off = d_level_off.as<uint32_t>();
     sa.li_off = d_li_off.as<uint32_t>();
     sa.li = d_li.as<uint32_t>();
     sa.fi_off = d_fi_off.as<uint32_t>();
@@ -202,6 +207,7 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     sa.type = d_type.as<uint8_t>();
     sa.inj = d_inj.as<InjRec>();
     sa.list = d_tune_list.as<uint32_t>();
+    sa.wait_ns = kWaitLimitNs;
     sa.n_list = (uint32_t)list.size();
     sa.subtiles = kTileWords / M;
     sa.max_gate_level = plan.max_gate_level;
@@ -255,9 +261,10 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (!has_ckt || !has_faults || !has_pats) throw StateError{"load circuit, faults and patterns first"};
   fsimb_opts o{};
   if (opts) {
-    if (opts->struct_size != 0 && opts->struct_size < sizeof(fsimb_opts))
-      throw ArgError{"fsimb_opts.struct_size too small"};
-    o = *opts;
+    // callers built against the layout before n_detect pass a shorter struct
+    const size_t min_size = offsetof(fsimb_opts, n_detect);
+    if (opts->struct_size != 0 && opts->struct_size < min_size) throw ArgError{"fsimb_opts.struct_size too small"};
+    std::memcpy(&o, opts, opts->struct_size ? std::min<size_t>(opts->struct_size, sizeof o) : sizeof o);
   }
   if (o.words_per_item && o.words_per_item != 1 && o.words_per_item != 2 && o.words_per_item != 4 &&
       o.words_per_item != 8)
@@ -265,6 +272,10 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (o.block_threads && (o.block_threads < 32 || o.block_threads > 1024 || o.block_threads % 32))
     throw ArgError{"block_threads must be 0 or a multiple of 32 in 32..1024"};
   if (o.ctas_per_sm > 8) throw ArgError{"ctas_per_sm must be 0..8"};
+  if (o.sweep_variant > 2) throw ArgError{"sweep_variant must be 0, 1 or 2"};
+  if (o.sweep_variant == 2 && o.words_per_item > 2)
+    throw ArgError{"the global-memory sweep takes 1 or 2 words per item"};
+  const uint32_t n_detect = std::max<uint32_t>(o.n_detect, 1);
   CK(cudaSetDevice(device));
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : stream;
   has_results = false;
@@ -306,12 +317,14 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     upload(d_traced, plan.traced, s);
     upload(d_inj, plan.sweeps, s);
     upload(d_exact, plan.exact_fault, s);
+    eflag_uploaded = false;
     plan_uploaded = true;
   }
   if (!pats_uploaded) {
     upload(d_pwords, pats.words, s);
     pats_uploaded = true;
   }
+  CK(cudaEventRecord(upload_ev, s));
   uint64_t launches = 1;  // results init
   d_good.ensure(tiles * N * kTileWords * 8);
   d_sens.ensure((size_t)N * kTileWords * 8);
@@ -332,53 +345,89 @@ void fsimb_handle::run(const fsimb_opts* opts) {
 
   // Sweep shape: explicit options, the autotuned shape of this plan, or the
   // default (the largest words per item that fits; two CTAs per SM when 8
-  // or 4 words per item leave room for them).
+  // or 4 words per item leave room for them).  Circuits whose live values
+  // do not fit in shared memory take the global-memory sweep.
   double tune_ms_now = 0;
   int M = 0, occ = 1, threads = 0;
-  const bool explicit_shape = o.words_per_item || o.block_threads || o.ctas_per_sm;
-  if (explicit_shape) {
-    M = (int)o.words_per_item;
-    occ = o.ctas_per_sm ? (int)o.ctas_per_sm : 1;
-    threads = (int)o.block_threads;
-  } else if (o.tune && n_sweeps && tiles) {
-    if (tuned_gen != plan_gen) {
-      const auto t0 = std::chrono::steady_clock::now();
-      tune_shape(s, widths, widest);
-      tune_ms_now = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  bool wide = o.sweep_variant == 2;
+  size_t vals_bytes = 0, smem = 0;
+  uint32_t rec_buf = 0;
+  const size_t share1 = sweep_smem_share(smem_optin, smem_per_sm, 1);
+  if (!wide && o.sweep_variant == 0 && n_sweeps &&
+      (plan.max_live > kMaxSlots || sweep_vals_bytes(plan.max_live, 1) > share1))
+    wide = true;  // no schedule can fit: skip building them
+  if (!wide && n_sweeps) {
+    try {
+      const bool explicit_shape = o.words_per_item || o.block_threads || o.ctas_per_sm;
+      if (explicit_shape) {
+        M = (int)o.words_per_item;
+        occ = o.ctas_per_sm ? (int)o.ctas_per_sm : 1;
+        threads = (int)o.block_threads;
+      } else if (o.tune && tiles) {
+        if (tuned_gen != plan_gen) {
+          const auto t0 = std::chrono::steady_clock::now();
+          tune_shape(s, widths, widest);
+          tune_ms_now =
+              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        M = tuned_M;
+        occ = tuned_occ;
+        threads = tuned_T;
+      } else {
+        default_shape(widths, widest, M, occ, threads);
+      }
+      const size_t budget = sweep_smem_share(smem_optin, smem_per_sm, occ);
+      const bool fixed_M = M != 0;
+      if (!M) {
+        M = 8;
+        while (M > 1 && sweep_vals_bytes(plan.max_live, M) > budget) M /= 2;
+      }
+      for (;;) {
+        use_schedule(M);
+        const bool fits = sched.max_live <= kMaxSlots && sweep_vals_bytes(sched.max_live, M) <= budget;
+        if (fits) break;
+        if (fixed_M || M == 1)
+          throw LimitError{"a sweep needs " + std::to_string(sched.max_live) +
+                           " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
+                           " at " + std::to_string(M) + " word(s) per item and " + std::to_string(occ) +
+                           " CTA(s) per SM"};
+        M /= 2;
+      }
+      vals_bytes = sweep_vals_bytes(sched.max_live, M);
+      rec_buf = (uint32_t)std::min<size_t>(std::max<uint32_t>(sched.max_block16, 1),
+                                           (budget - vals_bytes) / 32);
+      smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
+      if (!threads) threads = (int)pick_sweep_threads(widths, M);
+      threads = std::min<int>(threads, (int)sweep_max_threads(M));
+    } catch (const LimitError&) {
+      if (o.sweep_variant == 1) throw;
+      wide = true;
     }
-    M = tuned_M;
-    occ = tuned_occ;
-    threads = tuned_T;
-  } else {
-    default_shape(widths, widest, M, occ, threads);
   }
-  const size_t budget = sweep_smem_share(smem_optin, smem_per_sm, occ);
-  const bool fixed_M = M != 0;
-  if (!M) {
-    M = 8;
-    while (M > 1 && sweep_vals_bytes(plan.max_live, M) > budget) M /= 2;
-  }
-  for (;;) {
-    use_schedule(M);
-    const bool fits = sched.max_live <= kMaxSlots && sweep_vals_bytes(sched.max_live, M) <= budget;
-    if (fits) break;
-    if (fixed_M || M == 1)
-      throw LimitError{"a sweep needs " + std::to_string(sched.max_live) +
-                       " live values; shared memory holds " + std::to_string(budget / (8 * M)) +
-                       " at " + std::to_string(M) + " word(s) per item and " + std::to_string(occ) +
-                       " CTA(s) per SM"};
-    M /= 2;
-  }
-  const size_t vals_bytes = sweep_vals_bytes(sched.max_live, M);
-  const uint32_t rec_buf = (uint32_t)std::min<size_t>(widest, (budget - vals_bytes) / 32);
-  const size_t smem = std::max<size_t>(16, vals_bytes + (size_t)rec_buf * 32);
-  if (!threads) threads = (int)pick_sweep_threads(widths, M);
-  threads = std::min<int>(threads, (int)sweep_max_threads(M));
-  if (!sched_uploaded) {
-    upload(d_recs, sched.recs, s);
-    upload(d_li_off, sched.li_off, s);
-    upload(d_li, sched.li, s);
-    sched_uploaded = true;
+  int blocks = 0, occ_got = 0;
+  if (wide) {
+    M = o.words_per_item ? (int)o.words_per_item : 2;
+    threads = 256;
+    if (!eflag_uploaded) {
+      std::vector<uint8_t> fl(N, 0);
+      for (uint32_t e = plan.n_pi; e < N; ++e)
+        fl[e] = (uint8_t)((plan.gate_fo[e] || plan.po_drv[e]) ? 1 : 0) | (uint8_t)(plan.po_drv[e] ? 2 : 0);
+      upload(d_eflag, fl, s);
+      eflag_uploaded = true;
+    }
+    CK(sweep_wide_occupancy(M, &occ_got));
+    const uint64_t per_block = (uint64_t)N * M * 8;
+    const uint64_t cap = std::max<uint64_t>((uint64_t)n_sms, (4ull << 30) / std::max<uint64_t>(per_block, 1));
+    blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)n_sms * std::max(occ_got, 1), cap));
+    if (n_sweeps) d_gvals.ensure((size_t)blocks * per_block);
+  } else if (n_sweeps) {
+    if (!sched_uploaded) {
+      upload(d_recs, sched.blob, s);
+      upload(d_lvl, sched.lvl, s);
+      upload(d_li_off, sched.li_off, s);
+      upload(d_li, sched.li, s);
+      sched_uploaded = true;
+    }
   }
   CK(cudaMemsetAsync(d_queue.p, 0, std::max<uint64_t>(tiles, 1) * sizeof(int), s));
   CK(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
@@ -408,11 +457,12 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   good_P = pats.P;
   CK(cudaEventRecord(e2, s));
 
-  CK(sweep_set_smem(M, smem));
-  int occ_got = 0;
-  CK(sweep_occupancy(M, threads, smem, &occ_got));
-  if (occ_got < 1) throw LimitError{"sweep kernel does not fit on an SM with this shape"};
-  const int blocks = n_sms * occ_got;
+  if (!wide && n_sweeps) {
+    CK(sweep_set_smem(M, smem));
+    CK(sweep_occupancy(M, threads, smem, &occ_got));
+    if (occ_got < 1) throw LimitError{"sweep kernel does not fit on an SM with this shape"};
+    blocks = n_sms * occ_got;
+  }
 
   // 3. tiles
   uint32_t n_sw = n_sweeps, n_rt = n_roots, n_ex = n_exact;
@@ -429,31 +479,55 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     cudaEvent_t a0 = ev(4 + 3 * t), a1 = ev(5 + 3 * t), a2 = ev(6 + 3 * t);
     CK(cudaEventRecord(a0, s));
     if (n_sw) {
-      SweepArgs sa{};
-      sa.recs = d_recs.as<uint4>();
-      sa.level = d_level.as<uint32_t>();
-      sa.level_off = d_level_off.as<uint32_t>();
-      sa.li_off = d_li_off.as<uint32_t>();
-      sa.li = d_li.as<uint32_t>();
-      sa.fi_off = d_fi_off.as<uint32_t>();
-      sa.fi_idx = d_fi_idx.as<uint32_t>();
-      sa.type = d_type.as<uint8_t>();
-      sa.inj = d_inj.as<InjRec>();
-      sa.list = sw_list;
-      sa.n_list = n_sw;
-      sa.subtiles = kTileWords / M;
-      sa.max_gate_level = plan.max_gate_level;
-      sa.N = N;
-      sa.good = good_t;
-      sa.out = d_out.as<uint64_t>();
-      sa.queue = d_queue.as<int>() + t;
-      sa.vals_bytes = (uint32_t)vals_bytes;
-      sa.rec_buf = rec_buf;
-      sa.err = d_err.as<int>();
-      const int nb = (int)std::min<uint64_t>((uint64_t)blocks, (uint64_t)n_sw * sa.subtiles);
-      CK(launch_sweep(M, threads, nb, smem, sa, s));
+      const uint32_t subtiles = kTileWords / M;
+      const int nb = (int)std::min<uint64_t>((uint64_t)blocks, (uint64_t)n_sw * subtiles);
+      if (wide) {
+        SweepWideArgs wa{};
+        wa.level = d_level.as<uint32_t>();
+        wa.level_off = d_level_off.as<uint32_t>();
+        wa.fi_off = d_fi_off.as<uint32_t>();
+        wa.fi_idx = d_fi_idx.as<uint32_t>();
+        wa.type = d_type.as<uint8_t>();
+        wa.eflag = d_eflag.as<uint8_t>();
+        wa.inj = d_inj.as<InjRec>();
+        wa.list = sw_list;
+        wa.n_list = n_sw;
+        wa.subtiles = subtiles;
+        wa.max_gate_level = plan.max_gate_level;
+        wa.N = N;
+        wa.good = good_t;
+        wa.out = d_out.as<uint64_t>();
+        wa.queue = d_queue.as<int>() + t;
+        wa.gvals = d_gvals.as<uint64_t>();
+        CK(launch_sweep_wide(M, nb, wa, s));
+      } else {
+        SweepArgs sa{};
+        sa.blob = d_recs.as<uint4>();
+        sa.lvl = d_lvl.as<uint4>();
+        sa.level = d_level.as<uint32_t>();
+        sa.li_off = d_li_off.as<uint32_t>();
+        sa.li = d_li.as<uint32_t>();
+        sa.fi_off = d_fi_off.as<uint32_t>();
+        sa.fi_idx = d_fi_idx.as<uint32_t>();
+        sa.type = d_type.as<uint8_t>();
+        sa.inj = d_inj.as<InjRec>();
+        sa.list = sw_list;
+        sa.n_list = n_sw;
+        sa.subtiles = subtiles;
+        sa.max_gate_level = plan.max_gate_level;
+        sa.N = N;
+        sa.good = good_t;
+        sa.out = d_out.as<uint64_t>();
+        sa.queue = d_queue.as<int>() + t;
+        sa.vals_bytes = (uint32_t)vals_bytes;
+        sa.rec_buf = rec_buf;
+        sa.err = d_err.as<int>();
+        sa.wait_ns = o.wait_test ? kWaitTestNs : kWaitLimitNs;
+        sa.wait_test = (o.wait_test && t == 0) ? 1u : 0u;
+        CK(launch_sweep(M, threads, nb, smem, sa, s));
+      }
       ++launches;
-      items += (uint64_t)n_sw * sa.subtiles;
+      items += (uint64_t)n_sw * subtiles;
       if (!sw_list) {
         dense += plan.dense_sweep_gates * kTileWords;
         alg_bytes += plan.dense_sweep_bytes * kTileWords;
@@ -464,7 +538,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
         for (uint32_t si : host_sw) {
           uint32_t L0 = nl.level[plan.sweeps[si].elem] + 1;
           if (L0 <= plan.max_gate_level) {
-            dense += (uint64_t)(gates_end - plan.level_off[L0]) * kTileWords;
+            dense += (uint64_t)(plan.eval_prefix[gates_end] - plan.eval_prefix[plan.level_off[L0]]) * kTileWords;
             alg_bytes += (plan.nfp_prefix[gates_end] - plan.nfp_prefix[plan.level_off[L0]]) * kTileWords;
           }
         }
@@ -487,6 +561,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     fa.W = (uint32_t)W;
     fa.P = pats.P;
     fa.drop = o.drop ? 1 : 0;
+    fa.n_detect = n_detect;
     fa.count = d_count.as<unsigned long long>();
     fa.first = d_first.as<unsigned long long>();
     fa.lastflag = d_lastflag.as<uint8_t>();
@@ -502,6 +577,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
     xa.W = (uint32_t)W;
     xa.P = pats.P;
     xa.drop = o.drop ? 1 : 0;
+    xa.n_detect = n_detect;
     xa.count = fa.count;
     xa.first = fa.first;
     xa.lastflag = fa.lastflag;
@@ -522,6 +598,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
       da.n_exact_in = n_ex;
       da.first_exact_sweep = plan.n_stem_sweeps;
       da.count = d_count.as<unsigned long long>();
+      da.n_detect = n_detect;
       da.out_roots = d_root_list[cur].as<uint32_t>();
       da.out_sweeps = d_sweep_list.as<uint32_t>();
       da.out_exact = d_exact_list[cur].as<uint32_t>();
@@ -573,7 +650,7 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   }
   CK(cudaEventRecord(e4, s));
   CK(cudaStreamSynchronize(s));
-  if (kerr) throw CudaError{"a sweep kernel reached its wait limit for a record copy; results discarded"};
+  if (kerr) throw CudaError{"a sweep kernel reached its time limit waiting for a record copy; results discarded"};
   if (!o.drop) {
     for (uint64_t t = 0; t < tiles; ++t) {
       float x = 0;
@@ -619,15 +696,19 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   CK(cudaEventElapsedTime(&x, e1, e3));
   stats.ms_compute = x;
   stats.good_gate_words = (uint64_t)(N - plan.n_pi) * W_pad;
-  stats.max_live = sched.max_live;
-  stats.bank_conflict_groups = sched.conflict_groups;
-  stats.bank_access_groups = sched.access_groups;
+  stats.max_live = wide ? 0 : sched.max_live;
+  stats.bank_conflict_groups = wide ? 0 : sched.conflict_groups;
+  stats.bank_access_groups = wide ? 0 : sched.access_groups;
+  stats.sweep_variant = wide ? 2 : 1;
+  stats.hbm_bytes_per_tile = (uint64_t)N * kTileWords * 8 + (uint64_t)n_sweeps * (kTileWords * 8 + sizeof(InjRec)) +
+                             (wide ? (uint64_t)N * 10 + nl.fi_idx.size() * 4 : sched.bytes());
   stats.ms_tune = tune_ms_now;
   stats.ctas_per_sm = (uint32_t)occ_got;
   stats.words_per_item = (uint32_t)M;
   stats.block_threads = (uint32_t)threads;
   stats.blocks = (uint32_t)blocks;
   stats.smem_bytes = (uint32_t)smem;
+  (void)widest;
   stats.device_bytes = device_bytes();
 }
 
@@ -663,6 +744,7 @@ int fsimb_create(int device, fsimb_handle** out) {
       h->smem_optin = (size_t)optin;
       h->smem_per_sm = (size_t)per_sm;
       CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&h->upload_ev, cudaEventDisableTiming));
     }
   } catch (const CudaError& e) {
     g_create_error = e.msg;
@@ -1133,7 +1215,8 @@ __global__ void k_good_level_static(const uint8_t* type, const uint32_t* fi_off,
 }
 
 // Address of the static array on the current device, looked up once per
-// device (host code cannot use the array's name as a device address).
+// device (host code cannot use the array's name as a device address).  A
+// device reset ends the handles on that device and invalidates the address.
 uint64_t* noalloc_scratch(int device) {
   if (device < 0 || device >= kNoAllocMaxDevices) throw ArgError{"device index out of range"};
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
@@ -1161,6 +1244,8 @@ extern "C" int fsimb_good_po_noalloc(fsimb_handle* h, const uint64_t* d_pattern_
   CK(cudaSetDevice(h->device));
   uint64_t* vals = noalloc_scratch(h->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  // the circuit arrays were uploaded by the last fsimb_run, maybe on another stream
+  CK(cudaStreamWaitEvent(s, h->upload_ev, 0));
   const uint32_t po_begin = (uint32_t)(h->nl.n_pi + h->nl.n_gates);
   for (uint32_t l = 0; l < h->nl.n_levels; ++l) {
     const uint32_t lo = h->nl.level_off[l], hi = h->nl.level_off[l + 1];

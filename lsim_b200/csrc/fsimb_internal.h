@@ -195,14 +195,21 @@ struct fsimb_handle {
   uint64_t tuned_gen = 0;
   int tuned_M = 0, tuned_T = 0, tuned_occ = 0;
   cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+  // Recorded after each fsimb_run's uploads, on the run's stream: work on
+  // another stream that reads the circuit arrays waits for it.
+  cudaEvent_t upload_ev = nullptr;
 
   fsimb::DevBuf d_type, d_fi_off, d_fi_idx, d_recs, d_level, d_level_off, d_li_off, d_li;
+  fsimb::DevBuf d_lvl;     // schedule LevelDesc per level
+  fsimb::DevBuf d_eflag;   // wide-circuit sweep: per element, evaluated / drives a PO
+  fsimb::DevBuf d_gvals;   // wide-circuit sweep: per-CTA value regions
   fsimb::DevBuf d_roots, d_members, d_traced, d_inj, d_exact;
   fsimb::DevBuf d_pwords, d_good, d_out, d_sens, d_count, d_first, d_lastflag, d_queue, d_err;
   fsimb::DevBuf d_root_list[2], d_sweep_list, d_exact_list[2], d_nout, d_tune_list;
   uint64_t good_tiles = 0;  // tiles held in d_good
   uint64_t good_P = 0;
   bool pats_uploaded = false;  // d_pwords holds the current patterns
+  bool eflag_uploaded = false; // d_eflag holds the current plan's element flags
 
   std::vector<fsimb_fault_result> results;
   bool has_results = false;
@@ -213,7 +220,7 @@ struct fsimb_handle {
     if (device >= 0) {
       cudaSetDevice(device);
       for (fsimb::DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
-                        &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+                        &d_lvl, &d_eflag, &d_gvals, &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                         &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
                         &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
                         &d_exact_list[0], &d_exact_list[1], &d_nout, &d_tune_list})
@@ -221,6 +228,7 @@ struct fsimb_handle {
       for (auto e : events) cudaEventDestroy(e);
       for (auto e : tune_ev)
         if (e) cudaEventDestroy(e);
+      if (upload_ev) cudaEventDestroy(upload_ev);
       if (stream) cudaStreamDestroy(stream);
     }
   }
@@ -237,7 +245,7 @@ struct fsimb_handle {
   uint64_t device_bytes() const {
     uint64_t s = 0;
     for (const fsimb::DevBuf* b : {&d_type, &d_fi_off, &d_fi_idx, &d_recs, &d_level, &d_level_off,
-                            &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
+                            &d_lvl, &d_eflag, &d_gvals, &d_li_off, &d_li, &d_roots, &d_members, &d_traced, &d_inj, &d_exact,
                             &d_pwords, &d_good, &d_out, &d_sens, &d_count, &d_first, &d_lastflag,
                             &d_queue, &d_err, &d_root_list[0], &d_root_list[1], &d_sweep_list,
                             &d_exact_list[0], &d_exact_list[1], &d_nout, &d_tune_list})

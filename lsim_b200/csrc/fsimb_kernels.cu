@@ -114,17 +114,29 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-// Waits for the barrier's phase `parity` with an iteration limit; false if
-// the limit was reached (the caller reports the error instead of hanging).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 24); ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the barrier's phase `parity` for at most limit_ns nanoseconds of
+// the global timer (and at most 2^26 polls); false if it gave up, so the
+// caller reports an error instead of hanging.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -143,20 +155,21 @@ __device__ __forceinline__ uint32_t find_prefix(const unsigned long long* prefix
 // ---------------------------------------------------------------- sweep
 // Per-circuit pointers a sweep item reads (one circuit, one tile).
 struct SweepView {
-  const uint4* recs;
-  const uint32_t* level;
-  const uint32_t* level_off;
+  const uint4* blob;       // level blocks of gate records (fsimb_plan.h)
+  const uint4* lvl;        // LevelDesc per level
+  const uint32_t* level;   // element -> level
   const uint32_t* li_off;
-  const uint32_t* li;
+  const uint32_t* li;      // (element, slot) pairs
   const uint32_t* fi_off;
   const uint32_t* fi_idx;
   const uint8_t* type;
-  const uint64_t* good;  // tile [N][32]
+  const uint64_t* good;    // tile [N][32]
   uint32_t max_gate_level;
 };
 
 // Faulty value of the injection element for word w of the tile.
-__device__ __forceinline__ uint64_t inj_value(const SweepView& a, const InjRec& inj, uint32_t w) {
+template <class V>
+__device__ __forceinline__ uint64_t inj_value(const V& a, const InjRec& inj, uint32_t w) {
   const uint32_t x = inj.elem;
   if (!(inj.mode & kInjStuck)) return ~a.good[(uint64_t)x * 32 + w];
   const uint64_t sv = inj.value ? ~0ull : 0ull;
@@ -198,13 +211,94 @@ __device__ __forceinline__ void sts_chunk(uint64_t* vals, uint32_t slot, int h, 
 template <int M>
 using PoAcc = uint64_t[(M >= 2) ? M / 2 : 1][(M >= 2) ? 2 : 1];
 
+// ---- plain records: one compile-time body per gate class
+template <uint32_t CLS>
+__device__ __forceinline__ uint64_t plain_fn(uint64_t a, uint64_t b, uint64_t c) {
+  if constexpr (CLS == kPBuf) return a;
+  else if constexpr (CLS == kPInv) return ~a;
+  else if constexpr (CLS == kPAnd2) return a & b;
+  else if constexpr (CLS == kPNand2) return ~(a & b);
+  else if constexpr (CLS == kPOr2) return a | b;
+  else if constexpr (CLS == kPNor2) return ~(a | b);
+  else if constexpr (CLS == kPXor2) return a ^ b;
+  else if constexpr (CLS == kPXnor2) return ~(a ^ b);
+  else if constexpr (CLS == kPAnd3) return a & b & c;
+  else if constexpr (CLS == kPNand3) return ~(a & b & c);
+  else if constexpr (CLS == kPOr3) return a | b | c;
+  else if constexpr (CLS == kPNor3) return ~(a | b | c);
+  else if constexpr (CLS == kPXor3) return a ^ b ^ c;
+  else return ~(a ^ b ^ c);
+}
+
+// Slot chunk h of the value at byte offset `off` (slot * 8M).
+template <int M>
+__device__ __forceinline__ void ldo(const char* vb, uint32_t off, int h, uint64_t (&v)[2]) {
+  if constexpr (M == 1) {
+    v[0] = *reinterpret_cast<const uint64_t*>(vb + off);
+  } else {
+    const ulonglong2 q = *reinterpret_cast<const ulonglong2*>(vb + off + 16 * h);
+    v[0] = q.x;
+    v[1] = q.y;
+  }
+}
+template <int M>
+__device__ __forceinline__ void sto(char* vb, uint32_t off, int h, const uint64_t (&v)[2]) {
+  if constexpr (M == 1)
+    *reinterpret_cast<uint64_t*>(vb + off) = v[0];
+  else
+    *reinterpret_cast<ulonglong2*>(vb + off + 16 * h) = make_ulonglong2(v[0], v[1]);
+}
+
+// A plain record (fsimb_plan.h plain_rec) of class CLS on all M words.
+template <int M, uint32_t CLS>
+__device__ __forceinline__ void plain_body(char* vb, const uint2 r, int pl) {
+  constexpr int C = (M >= 2) ? M / 2 : 1;
+  constexpr int VC = (M >= 2) ? 2 : 1;
+  constexpr int NF = CLS <= kPInv ? 1 : (CLS <= kPXnor2 ? 2 : 3);
+  constexpr uint32_t SB = 8u * M;
+  const uint32_t o0 = (r.x & 0x7FFFu) * SB;
+  const uint32_t o1 = ((r.x >> 15) & 0x7FFFu) * SB;
+  const uint32_t o2 = (__funnelshift_r(r.x, r.y, 30) & 0x7FFFu) * SB;
+  const uint32_t oo = ((r.y >> 13) & 0x7FFFu) * SB;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int h = (C == 1) ? 0 : (pl + c) % C;
+    uint64_t a[2], b[2] = {0, 0}, d[2] = {0, 0}, o[2];
+    ldo<M>(vb, o0, h, a);
+    if constexpr (NF > 1) ldo<M>(vb, o1, h, b);
+    if constexpr (NF > 2) ldo<M>(vb, o2, h, d);
+#pragma unroll
+    for (int v = 0; v < VC; ++v) o[v] = plain_fn<CLS>(a[v], b[v], d[v]);
+    sto<M>(vb, oo, h, o);
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void plain_dispatch(char* vb, const uint2 r, int pl) {
+  switch (r.y >> 28) {  // class, sorted on the host so a warp mostly takes one case
+    case kPBuf: plain_body<M, kPBuf>(vb, r, pl); break;
+    case kPInv: plain_body<M, kPInv>(vb, r, pl); break;
+    case kPAnd2: plain_body<M, kPAnd2>(vb, r, pl); break;
+    case kPNand2: plain_body<M, kPNand2>(vb, r, pl); break;
+    case kPOr2: plain_body<M, kPOr2>(vb, r, pl); break;
+    case kPNor2: plain_body<M, kPNor2>(vb, r, pl); break;
+    case kPXor2: plain_body<M, kPXor2>(vb, r, pl); break;
+    case kPXnor2: plain_body<M, kPXnor2>(vb, r, pl); break;
+    case kPAnd3: plain_body<M, kPAnd3>(vb, r, pl); break;
+    case kPNand3: plain_body<M, kPNand3>(vb, r, pl); break;
+    case kPOr3: plain_body<M, kPOr3>(vb, r, pl); break;
+    case kPNor3: plain_body<M, kPNor3>(vb, r, pl); break;
+    case kPXor3: plain_body<M, kPXor3>(vb, r, pl); break;
+    case kPXnor3: plain_body<M, kPXnor3>(vb, r, pl); break;
+    default: break;  // kPNop
+  }
+}
+
+// ---- wide records (PO drivers, MUX, four inputs): runtime type and masks
 // One gate of a known class (family F, fan-in NF) on all M words of the item:
 // loads of the fanin chunks, the gate function, the store and the PO
 // difference.  F = 0: io ^ AND(in ^ ii) covers AND, NAND, OR, NOR, INV and
-// CLKBUF; F = 1: io ^ XOR(in) covers XOR and XNOR; F = 2: MUX.  Each class is
-// its own code path, selected by one branch per gate (gates are ordered by
-// class, so the branch is warp-uniform).  Loads and stores sit inside the
-// class bodies so that the branch stays a branch.
+// CLKBUF; F = 1: io ^ XOR(in) covers XOR and XNOR; F = 2: MUX.
 template <int M, int F, int NF>
 __device__ __forceinline__ void gate_body(uint64_t* vals, const uint4 q, uint32_t meta, int pl,
                                           const uint64_t* good_row, PoAcc<M>& pacc) {
@@ -290,6 +384,16 @@ __device__ __forceinline__ void gate_dispatch(uint64_t* vals, const uint4 q, int
   }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // M words per item, one thread per gate holding all M words.  Slots are
 // M*8 bytes; a thread reads a slot as C = M/2 16-byte chunks (one 8-byte word
 // for M = 1).  The host orders each level in groups of G = 16/M consecutive
@@ -299,43 +403,59 @@ __device__ __forceinline__ void gate_dispatch(uint64_t* vals, const uint4 q, int
 // phase touches lie in 8 different bank quads: the loads and stores of a
 // sweep are free of bank conflicts wherever the host found such groups.
 //
-// Gate records are staged per level into two shared-memory buffers by TMA
-// bulk copies issued two levels ahead (one elected thread, mbarrier
-// completion); a level wider than a buffer reads the rest from global.
+// Each level's block of gate records is staged into one of two shared-memory
+// buffers by a TMA bulk copy issued two levels ahead (one elected thread,
+// mbarrier completion, waits bounded in time); a block larger than a buffer
+// reads the rest from global memory.
 struct SweepCta {
   uint64_t* vals;     // [max_live][M]
   uint4* recbuf;      // [2][rec_buf]
-  uint64_t* bars;     // [2] mbarriers
+  uint64_t* bars;     // [3] mbarriers: two staging buffers, one for the wait test
   unsigned long long* acc;
-  uint32_t rec_buf;
-  uint32_t phase0, phase1;
+  uint32_t rec_buf;   // 16-byte units per staging buffer
+  uint32_t phase;     // bit b: next phase parity of staging barrier b
+  uint32_t issued;    // bit b: a copy into buffer b has not been waited for yet
+  uint64_t wait_ns;   // limit of one wait
+  uint32_t test_stall;
 };
 
 template <int M>
 __device__ __forceinline__ void sweep_cta_init(SweepCta& k, uint64_t* vals, uint32_t vals_bytes,
-                                               uint32_t rec_buf, uint64_t* bars, unsigned long long* acc) {
+                                               uint32_t rec_buf, uint64_t* bars, unsigned long long* acc,
+                                               uint64_t wait_ns, uint32_t test_stall) {
   k.vals = vals;
   k.recbuf = reinterpret_cast<uint4*>(reinterpret_cast<char*>(vals) + vals_bytes);
   k.bars = bars;
   k.acc = acc;
   k.rec_buf = rec_buf;
-  k.phase0 = k.phase1 = 0;
-  // Zeroed buffers: a record read before its copy landed names slot 0 and
-  // element 0, both in range.
-  for (uint32_t i = threadIdx.x; i < 2 * rec_buf; i += blockDim.x) k.recbuf[i] = make_uint4(0, 0, 0, 0);
+  k.phase = 0;
+  k.issued = 0;
+  k.wait_ns = wait_ns;
+  k.test_stall = test_stall;
   if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 }
 
+// Thread 0 only: the block of level L into buffer b.
 __device__ __forceinline__ void sweep_stage(SweepCta& k, const SweepView& v, uint32_t L, int b) {
-  const uint32_t lo = v.level_off[L], hi = v.level_off[L + 1];
-  const uint32_t n = min(hi - lo, k.rec_buf);
+  const uint4 d = v.lvl[L];
+  const uint32_t n = min(d.w, k.rec_buf);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  bulk_load(k.recbuf + (size_t)b * k.rec_buf, v.recs + lo, n * 16u, &k.bars[b]);
+  bulk_load(k.recbuf + (size_t)b * k.rec_buf, v.blob + d.x, n * 16u, &k.bars[b]);
+}
+
+// Error path: thread 0 waits (bounded) for the copies still in flight into
+// this CTA's shared memory, so none lands after the CTA has exited.
+__device__ __forceinline__ void sweep_drain(SweepCta& k) {
+  if (threadIdx.x == 0)
+    for (int b = 0; b < 2; ++b)
+      if ((k.issued >> b) & 1u) mbar_wait(&k.bars[b], (k.phase >> b) & 1u, k.wait_ns);
+  __syncthreads();
 }
 
 // One item: the levels above the injection element for M words starting at
@@ -353,36 +473,60 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
   const uint32_t my_off = (uint32_t)((tid & ~(PH - 1)) + ((M >= 2) ? (pl % C) * G + pl / C : pl));
   const uint32_t Lmax = v.max_gate_level;
   uint64_t* vals = k.vals;
+  char* vb = reinterpret_cast<char*>(vals);
   const uint32_t x = inj.elem;
   const uint32_t L0 = v.level[x] + 1;
   if (tid < M) k.acc[tid] = 0ull;
-  if (tid == 0 && L0 <= Lmax) {
-    sweep_stage(k, v, L0, 0);
-    if (L0 + 1 <= Lmax) sweep_stage(k, v, L0 + 1, 1);
-  }
-  uint32_t lo = 0, hi = 0;
   if (L0 <= Lmax) {
-    lo = v.level_off[L0];
-    hi = v.level_off[L0 + 1];
-    // Values live at the start level come from the good machine, except
-    // the injection element itself.
+    if (tid == 0) {
+      sweep_stage(k, v, L0, 0);
+      if (L0 + 1 <= Lmax) sweep_stage(k, v, L0 + 1, 1);
+    }
+    k.issued = (L0 + 1 <= Lmax) ? 3u : 1u;
+  }
+  bool ok = true;
+  if (k.test_stall) {
+    // test hook: wait on a barrier that no copy completes, so the wait runs
+    // out and the item takes the error path
+    k.test_stall = 0;
+    if (tid == 0) ok = mbar_wait(&k.bars[2], 0, k.wait_ns);
+  }
+  if (L0 <= Lmax) {
+    // Values live at the start level come from the good machine (copied
+    // asynchronously, four list entries in flight per thread), except the
+    // injection element itself.
     const uint32_t i1 = v.li_off[L0 + 1];
-    for (uint32_t i = v.li_off[L0] + tid; i < i1; i += nth) {
-      const uint2 es = reinterpret_cast<const uint2*>(v.li)[i];
-      uint64_t* dst = vals + (size_t)es.y * M;
-      if (es.x == x) {
+    const uint2* li = reinterpret_cast<const uint2*>(v.li);
+    for (uint32_t i = v.li_off[L0] + tid; i < i1; i += 4 * nth) {
+      uint2 es[4];
 #pragma unroll
-        for (int m = 0; m < M; ++m) dst[m] = inj_value(v, inj, w0 + m);
-      } else {
-        const uint64_t* src = v.good + (uint64_t)es.x * 32 + w0;
+      for (int j = 0; j < 4; ++j) es[j] = (i + j * nth < i1) ? li[i + j * nth] : make_uint2(0xFFFFFFFFu, 0);
 #pragma unroll
-        for (int m = 0; m < M; ++m) dst[m] = src[m];
+      for (int j = 0; j < 4; ++j) {
+        if (es[j].x == 0xFFFFFFFFu) continue;
+        uint64_t* dst = vals + (size_t)es[j].y * M;
+        if (es[j].x == x) {
+#pragma unroll
+          for (int m = 0; m < M; ++m) dst[m] = inj_value(v, inj, w0 + m);
+        } else {
+          const uint64_t* src = v.good + (uint64_t)es[j].x * 32 + w0;
+          if constexpr (M == 1) {
+            cp_async8(dst, src);
+          } else {
+#pragma unroll
+            for (int q = 0; q < M / 2; ++q) cp_async16(dst + 2 * q, src + 2 * q);
+          }
+        }
       }
     }
+    cp_async_wait_all();
   }
   if (tid < M && (inj.mode & kInjReachesPo))
     k.acc[tid] = inj_value(v, inj, w0 + tid) ^ v.good[(uint64_t)x * 32 + w0 + tid];
-  __syncthreads();
+  if (__syncthreads_or(!ok)) {
+    sweep_drain(k);
+    return false;
+  }
   PoAcc<M> pacc;
 #pragma unroll
   for (int c = 0; c < C; ++c)
@@ -390,21 +534,44 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
     for (int q = 0; q < VC; ++q) pacc[c][q] = 0ull;
   for (uint32_t L = L0; L <= Lmax; ++L) {
     const int b = (int)((L - L0) & 1u);
-    const uint32_t nhi = (L < Lmax) ? v.level_off[L + 2] : hi;  // used next level
-    const bool ok = mbar_wait(&k.bars[b], b ? k.phase1 : k.phase0);
-    if (b)
-      k.phase1 ^= 1u;
-    else
-      k.phase0 ^= 1u;
-    const uint4* rb = k.recbuf + (size_t)b * k.rec_buf;
-    for (uint32_t off = my_off; lo + off < hi; off += nth) {
-      const uint4 q = (off < k.rec_buf) ? rb[off] : v.recs[lo + off];
-      gate_dispatch<M>(vals, q, pl, v.good + (uint64_t)q.w * 32 + w0, pacc);
+    const uint4 desc = v.lvl[L];  // issued before the wait, used after it
+    ok = mbar_wait(&k.bars[b], (k.phase >> b) & 1u, k.wait_ns);
+    if (ok) {
+      k.phase ^= 1u << b;
+      k.issued &= ~(1u << b);
+      const char* sb = reinterpret_cast<const char*>(k.recbuf + (size_t)b * k.rec_buf);
+      const char* gb = reinterpret_cast<const char*>(v.blob + desc.x);
+      const uint32_t staged = min(desc.w, k.rec_buf) * 16u;
+      const uint32_t np = desc.y, n = desc.y + desc.z;
+      const uint32_t wide0 = (np + 1) / 2 * 16;
+      for (uint32_t p = my_off; p < n; p += nth) {
+        if (p < np) {
+          const uint32_t byte = p * 8;
+          uint2 r;
+          if (byte < staged)
+            r = *reinterpret_cast<const uint2*>(sb + byte);
+          else
+            r = *reinterpret_cast<const uint2*>(gb + byte);
+          plain_dispatch<M>(vb, r, pl);
+        } else {
+          const uint32_t byte = wide0 + (p - np) * 16;
+          uint4 q;
+          if (byte < staged)
+            q = *reinterpret_cast<const uint4*>(sb + byte);
+          else
+            q = *reinterpret_cast<const uint4*>(gb + byte);
+          gate_dispatch<M>(vals, q, pl, v.good + (uint64_t)q.w * 32 + w0, pacc);
+        }
+      }
     }
-    if (__syncthreads_or(!ok)) return false;
-    if (tid == 0 && L + 2 <= Lmax) sweep_stage(k, v, L + 2, b);
-    lo = hi;
-    hi = nhi;
+    if (__syncthreads_or(!ok)) {
+      sweep_drain(k);
+      return false;
+    }
+    if (L + 2 <= Lmax) {
+      if (tid == 0) sweep_stage(k, v, L + 2, b);
+      k.issued |= 1u << b;
+    }
   }
 #pragma unroll
   for (int c = 0; c < C; ++c) {
@@ -422,11 +589,12 @@ template <int M>
 __global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(SweepArgs a) {
   extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M] | recbuf[2][rec_buf]
   __shared__ unsigned long long acc[M];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[3];
   __shared__ int s_item;
   SweepCta k;
-  sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc);
-  const SweepView v{a.recs, a.level, a.level_off, a.li_off, a.li, a.fi_off, a.fi_idx, a.type, a.good,
+  sweep_cta_init<M>(k, vals, a.vals_bytes, a.rec_buf, bars, acc, a.wait_ns,
+                    (a.wait_test && blockIdx.x == 0) ? 1u : 0u);
+  const SweepView v{a.blob, a.lvl, a.level, a.li_off, a.li, a.fi_off, a.fi_idx, a.type, a.good,
                     a.max_gate_level};
   const uint32_t n_items = a.n_list * a.subtiles;
   for (;;) {
@@ -456,10 +624,10 @@ __global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64))
     k_sweep_batch(const __grid_constant__ BatchSweepParams p) {
   extern __shared__ __align__(16) uint64_t vals[];
   __shared__ unsigned long long acc[M];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[3];
   __shared__ uint32_t s_item;
   SweepCta k;
-  sweep_cta_init<M>(k, vals, p.vals_bytes, p.rec_buf, bars, acc);
+  sweep_cta_init<M>(k, vals, p.vals_bytes, p.rec_buf, bars, acc, p.wait_ns, 0u);
   constexpr uint32_t subtiles = kTileWords / M;
   for (uint32_t ci = 0; ci < p.n_circ; ++ci) {
     const SweepCirc& c = p.c[ci];
@@ -477,13 +645,78 @@ __global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64))
       const uint32_t rem = item - tile * per_tile;
       const uint32_t si = rem / subtiles;
       const uint32_t w0 = (rem % subtiles) * M;
-      const SweepView v{c.recs, c.level, c.level_off, c.li_off, c.li, c.fi_off, c.fi_idx, c.type,
+      const SweepView v{c.blob, c.lvl, c.level, c.li_off, c.li, c.fi_off, c.fi_idx, c.type,
                         c.good + (uint64_t)tile * c.N * 32, c.max_gate_level};
       if (!sweep_item<M>(k, v, c.inj[si], w0, c.out + ((uint64_t)tile * c.n_sweeps + si) * 32)) {
         if (threadIdx.x == 0) atomicExch(p.err, 1);
         return;
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------- wide circuits
+// Sweep for circuits whose live values do not fit in shared memory: every
+// CTA keeps the values of its item in its own region of global memory,
+// indexed by element (gvals + block * N * M), which L2 mostly holds.  A
+// fanin below the start level other than the injection element reads the
+// good machine directly, so an item starts without copying live values.
+// Threads take (element, word) pairs of a level; one barrier per level.
+template <int M>
+__global__ void __launch_bounds__(256) k_sweep_wide(SweepWideArgs a) {
+  __shared__ unsigned long long acc[M];
+  __shared__ uint32_t s_item;
+  uint64_t* gv = a.gvals + (size_t)blockIdx.x * a.N * M;
+  const uint32_t tid = threadIdx.x, nth = blockDim.x;
+  const uint32_t m = tid % M, step = nth / M;
+  const uint32_t n_items = a.n_list * a.subtiles;
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(a.queue, 1);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= n_items) return;
+    const uint32_t li = item / a.subtiles;
+    const uint32_t w0 = (item % a.subtiles) * M;
+    const uint32_t si = a.list ? a.list[li] : li;
+    const InjRec inj = a.inj[si];
+    const uint32_t x = inj.elem;
+    const uint32_t L0 = a.level[x] + 1;
+    const uint32_t lo0 = L0 <= a.max_gate_level ? a.level_off[L0] : 0;
+    if (tid < M) {
+      const uint64_t fv = inj_value(a, inj, w0 + tid);
+      gv[(size_t)x * M + tid] = fv;
+      acc[tid] = (inj.mode & kInjReachesPo) ? fv ^ a.good[(uint64_t)x * 32 + w0 + tid] : 0ull;
+    }
+    __syncthreads();
+    uint64_t pacc = 0;
+    const uint32_t w = w0 + m;
+    for (uint32_t L = L0; L <= a.max_gate_level; ++L) {
+      const uint32_t lo = a.level_off[L], hi = a.level_off[L + 1];
+      for (uint32_t e = lo + tid / M; e < hi; e += step) {
+        const uint8_t fl = a.eflag[e];
+        if (!(fl & 1u)) continue;
+        const uint8_t t = a.type[e];
+        const uint32_t f0 = a.fi_off[e];
+        uint32_t nf = a.fi_off[e + 1] - f0;
+        if (t == G_INV || t == G_CLKBUF || t == G_PO) nf = 1;
+        uint64_t in[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if ((uint32_t)q < nf) {
+            const uint32_t f = a.fi_idx[f0 + q];
+            in[q] = (f < lo0 && f != x) ? a.good[(uint64_t)f * 32 + w] : gv[(size_t)f * M + m];
+          }
+        }
+        const uint64_t r = eval_word(t, nf, in[0], in[1], in[2], in[3]);
+        gv[(size_t)e * M + m] = r;
+        if (fl & 2u) pacc |= r ^ a.good[(uint64_t)e * 32 + w];
+      }
+      __syncthreads();
+    }
+    if (pacc) atomicOr(&acc[m], (unsigned long long)pacc);
+    __syncthreads();
+    if (tid < M) a.out[(uint64_t)si * 32 + w0 + tid] = acc[tid];
   }
 }
 
@@ -543,7 +776,6 @@ __global__ void __launch_bounds__(256) k_ffr(FfrArgs a) {
   else
     obs = a.obs[(uint64_t)rr.obs * 32 + lane];
   obs &= mask;
-  const uint64_t tile_first = (uint64_t)a.tile * 32 * 64;
   a.sens[(uint64_t)rr.root * 32 + lane] = ~0ull;
   for (uint32_t i = rr.mem_begin; i < rr.mem_end; ++i) {
     const MemberRec m = a.members[i];
@@ -552,7 +784,7 @@ __global__ void __launch_bounds__(256) k_ffr(FfrArgs a) {
   }
   for (uint32_t i = rr.flt_begin; i < rr.flt_end; ++i) {
     const TracedRec tr = a.traced[i];
-    if (a.drop && a.first[tr.fault] < tile_first) continue;  // dropped earlier
+    if (a.drop && a.count[tr.fault] >= a.n_detect) continue;  // dropped after an earlier tile
     uint64_t s, gv;
     if (tr.pin == 0) {
       s = a.sens[(uint64_t)tr.elem * 32 + lane];
@@ -573,8 +805,7 @@ __global__ void __launch_bounds__(256) k_exact(ExactArgs a) {
   if (warp >= a.n_exact) return;
   const uint32_t j = a.list ? a.list[warp] : warp;
   const uint32_t f = a.exact_fault[j];
-  const uint64_t tile_first = (uint64_t)a.tile * 32 * 64;
-  if (a.drop && a.first[f] < tile_first) return;
+  if (a.drop && a.count[f] >= a.n_detect) return;  // dropped after an earlier tile
   const uint32_t w = a.tile * 32 + lane;
   const uint32_t bits = round_bits(a.P, a.W, w);
   const uint64_t mask = bits_mask(bits);
@@ -707,7 +938,7 @@ __global__ void k_drop(DropArgs a) {
       id = a.in_list ? a.in_list[i] : i;
       const RootRec rr = a.roots[id];
       for (uint32_t k = rr.flt_begin; k < rr.flt_end && !keep; ++k)
-        keep = a.count[a.traced[k].fault] == 0ull;
+        keep = a.count[a.traced[k].fault] < a.n_detect;
       sweep = keep && rr.obs != kObsOne && rr.obs != kObsZero;
       sw = rr.obs;
     }
@@ -715,7 +946,7 @@ __global__ void k_drop(DropArgs a) {
     const uint32_t j = i - a.n_in_pad;
     if (j < a.n_exact_in) {
       id = a.exact_in ? a.exact_in[j] : j;
-      keep = a.count[a.exact_fault[id]] == 0ull;
+      keep = a.count[a.exact_fault[id]] < a.n_detect;
       sweep = keep;
       sw = a.first_exact_sweep + id;
     }
@@ -827,6 +1058,23 @@ cudaError_t launch_sweep(int M, int threads, int blocks, size_t smem, const Swee
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_wide(int M, int blocks, const SweepWideArgs& a, cudaStream_t s) {
+  switch (M) {
+    case 1: k_sweep_wide<1><<<blocks, 256, 0, s>>>(a); break;
+    case 2: k_sweep_wide<2><<<blocks, 256, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t sweep_wide_occupancy(int M, int* blocks_per_sm) {
+  switch (M) {
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_sweep_wide<1>, 256, 0);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_sweep_wide<2>, 256, 0);
+  }
+  return cudaErrorInvalidValue;
 }
 
 void launch_ffr(const FfrArgs& a, cudaStream_t s) {

@@ -22,9 +22,9 @@ struct GoodArgs {
 };
 
 struct SweepArgs {
-  const uint4* recs;       // SweepRec per position (see fsimb_plan.h)
-  const uint32_t* level;
-  const uint32_t* level_off;
+  const uint4* blob;       // level blocks of gate records (see fsimb_plan.h)
+  const uint4* lvl;        // LevelDesc per level
+  const uint32_t* level;   // element -> level
   const uint32_t* li_off;
   const uint32_t* li;      // (element, slot) pairs
   const uint32_t* fi_off;
@@ -40,8 +40,30 @@ struct SweepArgs {
   uint64_t* out;           // this tile: [n_sweeps][32] OR of PO differences
   int* queue;              // work counter for this launch
   uint32_t vals_bytes;     // shared memory for values (multiple of 16)
-  uint32_t rec_buf;        // records per staging buffer (2 buffers follow the values)
+  uint32_t rec_buf;        // 16-byte units per staging buffer (2 buffers follow the values)
   int* err;                // set to 1 if a bounded wait gave up
+  uint64_t wait_ns;        // time limit of one wait for a record copy
+  uint32_t wait_test;      // 1: the first CTA waits on a barrier no copy completes (test hook)
+};
+
+// Sweep of circuits whose live values do not fit in shared memory.
+struct SweepWideArgs {
+  const uint32_t* level;     // element -> level
+  const uint32_t* level_off; // element offsets per level
+  const uint32_t* fi_off;
+  const uint32_t* fi_idx;
+  const uint8_t* type;
+  const uint8_t* eflag;      // bit 0: evaluated in sweeps, bit 1: drives a PO
+  const InjRec* inj;
+  const uint32_t* list;      // sweep indices to run (nullptr: 0..n_list-1)
+  uint32_t n_list;
+  uint32_t subtiles;         // 32 / M
+  uint32_t max_gate_level;
+  uint32_t N;
+  const uint64_t* good;      // this tile: [N][32]
+  uint64_t* out;             // this tile: [n_sweeps][32]
+  int* queue;
+  uint64_t* gvals;           // [blocks][N][M] values of each CTA's item
 };
 
 struct FfrArgs {
@@ -58,7 +80,8 @@ struct FfrArgs {
   uint64_t* sens;          // scratch [N][32]
   uint32_t tile, W;
   uint64_t P;
-  int drop;                // skip faults detected in an earlier tile
+  int drop;                // skip faults whose count reached n_detect in an earlier tile
+  uint32_t n_detect;       // >= 1
   unsigned long long* count;
   unsigned long long* first;
   uint8_t* lastflag;
@@ -73,6 +96,7 @@ struct ExactArgs {
   uint32_t tile, W;
   uint64_t P;
   int drop;
+  uint32_t n_detect;
   unsigned long long* count;
   unsigned long long* first;
   uint8_t* lastflag;
@@ -89,6 +113,7 @@ struct DropArgs {
   uint32_t n_exact_in;
   uint32_t first_exact_sweep;
   const unsigned long long* count;
+  uint32_t n_detect;         // a fault survives while its count is below this
   uint32_t* out_roots;       // surviving root indices
   uint32_t* out_sweeps;      // sweeps still needed (stem flips and exact faults)
   uint32_t* out_exact;       // surviving exact indices
@@ -99,9 +124,9 @@ struct DropArgs {
 // One circuit of a batch: device pointers into the batch's concatenated
 // arrays and the circuit's sizes.
 struct BatchCirc {
-  const uint4* recs;
+  const uint4* blob;
+  const uint4* lvl;
   const uint32_t* level;
-  const uint32_t* level_off;
   const uint32_t* li_off;
   const uint32_t* li;
   const uint32_t* fi_off;
@@ -130,9 +155,9 @@ struct BatchCirc {
 // What the batched sweep reads of one circuit.  A launch carries these in
 // its parameters, so the compiler sees them as warp-uniform values.
 struct SweepCirc {
-  const uint4* recs;
+  const uint4* blob;
+  const uint4* lvl;
   const uint32_t* level;
-  const uint32_t* level_off;
   const uint32_t* li_off;
   const uint32_t* li;
   const uint32_t* fi_off;
@@ -151,6 +176,7 @@ struct BatchSweepParams {
   SweepCirc c[kSweepCircsPerLaunch];
   unsigned long long* queue;  // [n_circ] work counters, zero before the launch
   int* err;
+  uint64_t wait_ns;
   uint32_t n_circ, vals_bytes, rec_buf;
 };
 static_assert(sizeof(BatchSweepParams) <= 32000, "kernel parameters are limited to 32,764 bytes");
@@ -187,6 +213,12 @@ cudaError_t launch_sweep(int M, int threads, int blocks, size_t smem, const Swee
                          cudaStream_t s);
 cudaError_t sweep_set_smem(int M, size_t smem);
 cudaError_t sweep_occupancy(int M, int threads, size_t smem, int* blocks_per_sm);
+// M in {1, 2}; 256 threads per CTA.
+cudaError_t launch_sweep_wide(int M, int blocks, const SweepWideArgs& a, cudaStream_t s);
+cudaError_t sweep_wide_occupancy(int M, int* blocks_per_sm);
+// Time limit of one wait for a record copy, and the shorter one of the wait test.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+constexpr uint64_t kWaitTestNs = 20000000ull;
 void launch_ffr(const FfrArgs& a, cudaStream_t s);
 void launch_exact(const ExactArgs& a, cudaStream_t s);
 void launch_init_results(unsigned long long* count, unsigned long long* first, uint8_t* lastflag,

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <array>
+#include <cstring>
+#include <functional>
 
 namespace fsimb {
 
@@ -25,6 +27,27 @@ uint32_t gate_class(uint8_t type, uint32_t nf) {
   if (fam == 1 && nf >= 2 && nf <= 4) return 4 + nf - 2;
   if (fam == 2 && nf == 3) return 7;
   return kClassGeneric;
+}
+
+uint32_t plain_class(uint8_t t, uint32_t nf) {
+  if (nf == 1) {
+    switch (t) {
+      case G_AND: case G_OR: case G_XOR: case G_CLKBUF: return kPBuf;
+      case G_INV: case G_NAND: case G_NOR: case G_XNOR: return kPInv;
+      default: return kPlainClasses;
+    }
+  }
+  if (nf != 2 && nf != 3) return kPlainClasses;
+  const uint32_t base = nf == 2 ? kPAnd2 : kPAnd3;
+  switch (t) {
+    case G_AND: return base + 0;
+    case G_NAND: return base + 1;
+    case G_OR: return base + 2;
+    case G_NOR: return base + 3;
+    case G_XOR: return base + 4;
+    case G_XNOR: return base + 5;
+    default: return kPlainClasses;
+  }
 }
 
 uint32_t gate_family(uint8_t t) {
@@ -121,11 +144,15 @@ void build_circuit_plan(const Netlist& nl, CircuitPlan& C) {
   }
 
   // Algorithmic bytes of one gate-word evaluation: its fanin words read and
-  // its output word written, 8 * (fanin + 1).
+  // its output word written, 8 * (fanin + 1).  A sweep evaluates the gates
+  // that feed a gate or a PO; gates that feed nothing cannot change a PO.
   P.nfp_prefix.assign(N + 1, 0);
+  P.eval_prefix.assign(N + 1, 0);
   for (uint32_t e = 0; e < N; ++e) {
-    uint32_t nf = e < P.n_pi ? 0 : eff_fanin(nl, e);
-    P.nfp_prefix[e + 1] = P.nfp_prefix[e] + 8ull * (nf + 1);
+    const bool ev = e >= P.n_pi && (P.gate_fo[e] || P.po_drv[e]);
+    const uint32_t nf = ev ? eff_fanin(nl, e) : 0;
+    P.nfp_prefix[e + 1] = P.nfp_prefix[e] + (ev ? 8ull * (nf + 1) : 0);
+    P.eval_prefix[e + 1] = P.eval_prefix[e] + (ev ? 1 : 0);
   }
 }
 
@@ -215,7 +242,7 @@ void build_fault_plan(const Netlist& nl, const CircuitPlan& C, const std::vector
   for (auto& s : P.sweeps) {
     uint32_t L0 = nl.level[s.elem] + 1;
     if (L0 <= P.max_gate_level) {
-      P.dense_sweep_gates += gates_end - nl.level_off[L0];
+      P.dense_sweep_gates += B.eval_prefix[gates_end] - B.eval_prefix[nl.level_off[L0]];
       P.dense_sweep_bytes += B.nfp_prefix[gates_end] - B.nfp_prefix[nl.level_off[L0]];
     }
   }
@@ -229,6 +256,7 @@ void build_plan(const Netlist& nl, const std::vector<Fault>& faults, Plan& P) {
   P.gate_fo = std::move(C.base.gate_fo);
   P.po_drv = std::move(C.base.po_drv);
   P.nfp_prefix = std::move(C.base.nfp_prefix);
+  P.eval_prefix = std::move(C.base.eval_prefix);
 }
 
 // ---------------------------------------------------------------- schedule
@@ -267,7 +295,6 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
     slot[e] = pool.alloc(rr++ % G);
     release[P.maxfo_level[e] + 1].push_back(slot[e]);
   }
-  S.recs.assign(N, SweepRec{});
   auto nf_of = [&](uint32_t e) { return std::min<uint32_t>(eff_fanin(nl, e), 4); };
   // Classes by (gate family, fan-in): a warp runs one code path.  The AND
   // family (AND, NAND, OR, NOR, INV, CLKBUF) is io ^ AND(in ^ ii), the XOR
@@ -366,32 +393,84 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       for (size_t c = 0; c < pool_in.size(); ++c)
         if (!taken[c]) leftover.push_back(pool_in[c]);
   };
+  S.lvl.assign(nl.n_levels + 1, LevelDesc{0, 0, 0, 0});
+  std::vector<uint64_t>& blob = S.blob;
+  std::vector<uint32_t> plain, wide;
   for (uint32_t L = 1; L <= P.max_gate_level && L < nl.n_levels; ++L) {
     for (uint32_t s : release[L]) pool.release(s);
     const uint32_t lo = nl.level_off[L], hi = nl.level_off[L + 1];
-    std::vector<uint32_t> elems(hi - lo);
-    for (uint32_t i = 0; i < hi - lo; ++i) elems[i] = lo + i;
-    std::stable_sort(elems.begin(), elems.end(),
-                     [&](uint32_t a, uint32_t b) { return cls_of(a) < cls_of(b); });
-    order.clear();
-    leftover.clear();
-    for (size_t i = 0; i < elems.size();) {
-      size_t j = i;
-      while (j < elems.size() && cls_of(elems[j]) == cls_of(elems[i])) ++j;
-      std::vector<uint32_t> cls(elems.begin() + i, elems.begin() + j);
-      make_groups(cls, false);
-      i = j;
+    // Gates that feed a gate or a PO; a plain record holds a gate that feeds
+    // gates only, with a compile-time class.
+    plain.clear();
+    wide.clear();
+    for (uint32_t e = lo; e < hi; ++e) {
+      if (!P.gate_fo[e] && !P.po_drv[e]) continue;
+      if (!P.po_drv[e] && plain_class(nl.type[e], nf_of(e)) < kPlainClasses)
+        plain.push_back(e);
+      else
+        wide.push_back(e);
     }
-    std::stable_sort(leftover.begin(), leftover.end(),
-                     [&](uint32_t a, uint32_t b) { return cls_of(a) < cls_of(b); });
-    make_groups(leftover, true);
+    order.clear();
+    // Groups of G inside each class, then the classes' partial groups as a
+    // mixed tail (grouped too); `key` orders the classes.
+    auto part = [&](std::vector<uint32_t>& elems, const std::function<uint32_t(uint32_t)>& key) {
+      std::stable_sort(elems.begin(), elems.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
+      leftover.clear();
+      for (size_t i = 0; i < elems.size();) {
+        size_t j = i;
+        while (j < elems.size() && key(elems[j]) == key(elems[i])) ++j;
+        std::vector<uint32_t> cls(elems.begin() + i, elems.begin() + j);
+        make_groups(cls, false);
+        i = j;
+      }
+      std::stable_sort(leftover.begin(), leftover.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
+      make_groups(leftover, true);
+    };
+    part(plain, [&](uint32_t e) { return plain_class(nl.type[e], nf_of(e)); });
+    uint32_t n_plain = (uint32_t)order.size();
+    // the wide part starts on a group boundary: pad with no-op records
+    const uint32_t n_pad = wide.empty() ? 0 : (G - n_plain % G) % G;
+    part(wide, [&](uint32_t e) { return cls_of(e); });
+    const uint32_t n_wide = (uint32_t)order.size() - n_plain;
+    // Level block: plain records (8 bytes), padded to 16 bytes, then wide
+    // records (16 bytes).
+    while (blob.size() % 2) blob.push_back(0);
+    LevelDesc& d = S.lvl[L];
+    d.off16 = (uint32_t)(blob.size() / 2);
+    d.n_plain = n_plain + n_pad;
+    d.n_wide = n_wide;
+    const size_t plain_base = blob.size();
+    blob.resize(plain_base + ((size_t)d.n_plain + 1) / 2 * 2 + 2ull * n_wide, 0);
+    for (uint32_t k = 0; k < n_pad; ++k) blob[plain_base + n_plain + k] = plain_rec(0, 0, 0, 0, kPNop);
+    const size_t wide_base = plain_base + ((size_t)d.n_plain + 1) / 2 * 2;
+    d.n16 = (uint32_t)((blob.size() - plain_base) / 2);
+    S.max_block16 = std::max(S.max_block16, d.n16);
     // Positions, output slots (residue = position mod G) and records.
+    std::vector<uint32_t> pos_slot[5];
+    for (auto& v : pos_slot) v.assign(order.size() + n_pad, kNoSlot);
     for (uint32_t o = 0; o < order.size(); ++o) {
       const uint32_t e = order[o];
-      SweepRec r{};
+      const uint32_t pos = o < n_plain ? o : o + n_pad;
       const uint32_t nf = nf_of(e);
-      for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)slot[nl.fi_idx[nl.fi_off[e] + perm[e][k]]];
+      uint32_t fs[4] = {0, 0, 0, 0};
+      for (uint32_t k = 0; k < nf; ++k) {
+        fs[k] = slot[nl.fi_idx[nl.fi_off[e] + perm[e][k]]];
+        pos_slot[k][pos] = fs[k];
+      }
+      uint32_t out = 0;
+      if (P.gate_fo[e]) {
+        slot[e] = pool.alloc(pos % G);
+        release[P.maxfo_level[e] + 1].push_back(slot[e]);
+        out = slot[e];
+        pos_slot[4][pos] = out;
+      }
       const uint8_t t = nl.type[e];
+      if (o < n_plain) {
+        blob[plain_base + o] = plain_rec(fs[0], fs[1], fs[2], out, plain_class(t, nf));
+        continue;
+      }
+      SweepRec r{};
+      for (uint32_t k = 0; k < nf; ++k) r.fs[k] = (uint16_t)fs[k];
       uint32_t meta = (uint32_t)t & kRecTypeMask;
       meta |= ((nf ? nf - 1 : 0) & 3u) << kRecNfShift;
       meta |= gate_class(t, nf) << kRecClassShift;
@@ -399,34 +478,26 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       if (t == G_INV || t == G_OR || t == G_NAND || t == G_XNOR) meta |= kRecIo;
       if (P.po_drv[e]) meta |= kRecPo;
       if (P.gate_fo[e]) {
-        slot[e] = pool.alloc(o % G);
-        release[P.maxfo_level[e] + 1].push_back(slot[e]);
         meta |= kRecHasSlot;
-        r.slot = (uint16_t)slot[e];
+        r.slot = (uint16_t)out;
       }
       r.meta = (uint16_t)meta;
       r.elem = e;
-      S.recs[lo + o] = r;
+      std::memcpy(&blob[wide_base + 2ull * (o - n_plain)], &r, sizeof r);
     }
     // Bank-conflict accounting per aligned group of G positions.
-    for (uint32_t g0 = 0; g0 < order.size(); g0 += G) {
-      const uint32_t g1 = std::min<uint32_t>(g0 + G, (uint32_t)order.size());
+    const uint32_t n_pos = (uint32_t)order.size() + n_pad;
+    for (uint32_t g0 = 0; g0 < n_pos; g0 += G) {
+      const uint32_t g1 = std::min<uint32_t>(g0 + G, n_pos);
       for (uint32_t k = 0; k < 5; ++k) {
         uint32_t seen = 0, any = 0;
         bool conflict = false;
         for (uint32_t o = g0; o < g1; ++o) {
-          const SweepRec& r = S.recs[lo + o];
-          uint32_t s;
-          if (k < 4) {
-            if (k >= ((r.meta >> kRecNfShift) & 3u) + 1u) continue;
-            s = r.fs[k];
-          } else {
-            if (!(r.meta & kRecHasSlot)) continue;
-            s = r.slot;
-          }
+          const uint32_t sl = pos_slot[k][o];
+          if (sl == kNoSlot) continue;
           any = 1;
-          conflict |= (seen >> (s % G)) & 1u;
-          seen |= 1u << (s % G);
+          conflict |= (seen >> (sl % G)) & 1u;
+          seen |= 1u << (sl % G);
         }
         S.access_groups += any;
         S.conflict_groups += conflict;
@@ -434,7 +505,10 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
     }
   }
   S.max_live = pool.next_block * G;
-  if (S.max_live > kMaxSlots) return;
+  if (S.max_live > kMaxSlots) {
+    S.blob.clear();
+    return;
+  }
   // Live-in sets as (element, slot) pairs.
   std::vector<uint32_t> cnt(nl.n_levels + 2, 0);
   for (uint32_t e = 0; e < N; ++e)

@@ -4,14 +4,22 @@
 // Layout in HBM (all arrays indexed by the reference's topological index):
 //   type[N]            u8 gate type
 //   fi_off[N+1], fi_idx[E]   fanin CSR in pin order (good-machine kernel)
-//   sweep_rec[N]       16-byte record per position of the sweep order: the
-//                      shared-memory slots of up to 4 fanins, the own slot,
-//                      type / fan-in / flags and the element index.  Within a
-//                      level the order is by gate class (family, fan-in), and
-//                      every group of G consecutive positions has pairwise
-//                      different slot residues mod G for each fanin and for
-//                      the output wherever the host found such groups, so the
-//                      group's shared-memory accesses hit distinct banks
+//   sweep blocks       per level one block of gate records (the level's
+//                      order of evaluation), 16-byte aligned:
+//                        plain records, 8 bytes: 15-bit shared-memory slots
+//                        of up to three fanins and of the output, and a
+//                        4-bit gate class (PlainClass) -- every non-MUX gate
+//                        with 1-3 inputs that feeds other gates and no PO;
+//                        wide records, 16 bytes (SweepRec): everything else
+//                        that must be evaluated (PO drivers, MUX, 4 inputs).
+//                      Gates that feed nothing are left out.  Within each
+//                      part the order is by class, and every group of G
+//                      consecutive positions has pairwise different slot
+//                      residues mod G for each fanin and for the output
+//                      wherever the host found such groups, so the group's
+//                      shared-memory accesses hit distinct banks
+//   lvl[L]             (block offset in 16-byte units, plain count, wide
+//                      count, block size in 16-byte units)
 //   li_off[L+1], li[]  (element, slot) pairs live when a sweep starts at
 //                      level L (read from the good values at start)
 //   good[tile][N][32]  u64 good-machine words, 32 words (2048 patterns) per tile
@@ -37,7 +45,30 @@ namespace fsimb {
 
 constexpr uint32_t kTileWords = 32;  // words per tile = lanes of a warp
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
-constexpr uint32_t kMaxSlots = 65535;   // slots are 16-bit in the sweep records
+constexpr uint32_t kMaxSlots = 32767;   // slots are 15-bit in the plain gate records
+
+// Plain gate records: classes of the gate function (a compile-time body in
+// the sweep kernel each).  One-input gates are BUF (AND, OR, XOR, CLKBUF) or
+// INV (INV, NAND, NOR, XNOR).  kPNop pads a level's plain part to a group
+// boundary and does nothing.
+enum PlainClass : uint32_t {
+  kPBuf = 0, kPInv, kPAnd2, kPNand2, kPOr2, kPNor2, kPXor2, kPXnor2,
+  kPAnd3, kPNand3, kPOr3, kPNor3, kPXor3, kPXnor3, kPlainClasses, kPNop = 15
+};
+// Bits [0,15) fanin 0, [15,30) fanin 1, [30,45) fanin 2, [45,60) output
+// slot, [60,64) class.
+inline uint64_t plain_rec(uint32_t f0, uint32_t f1, uint32_t f2, uint32_t out, uint32_t cls) {
+  return (uint64_t)f0 | ((uint64_t)f1 << 15) | ((uint64_t)f2 << 30) | ((uint64_t)out << 45) |
+         ((uint64_t)cls << 60);
+}
+
+// One level of the sweep order (see "sweep blocks" above).
+struct LevelDesc {
+  uint32_t off16;    // block offset in 16-byte units
+  uint32_t n_plain;  // plain records (8 bytes each, first)
+  uint32_t n_wide;   // wide records (16 bytes each, after the plain part padded to 16 bytes)
+  uint32_t n16;      // block size in 16-byte units
+};
 
 // SweepRec::meta bit fields
 constexpr uint32_t kRecTypeMask = 15u;     // bits 0-3: gate type
@@ -59,7 +90,7 @@ constexpr uint32_t kInjReachesPo = 2u;  // the element is, or drives, a PO
 constexpr uint32_t kObsZero = 0xFFFFFFFEu;  // root reaches no PO
 constexpr uint32_t kObsOne = 0xFFFFFFFFu;   // root is / drives a PO
 
-struct SweepRec {
+struct SweepRec {  // wide gate record
   uint16_t fs[4];  // fanin slots
   uint16_t slot;   // own slot (valid with kRecHasSlot)
   uint16_t meta;
@@ -107,7 +138,10 @@ struct Plan {
   uint32_t max_level_width = 0;
   uint64_t dense_sweep_gates = 0;    // sum over sweeps of gates evaluated
   uint64_t dense_sweep_bytes = 0;    // sum over sweeps of 8*(fanin+1) per evaluated gate, per word
-  std::vector<uint64_t> nfp_prefix;  // [N+1] prefix sums of 8*(effective fanin+1)
+  // [N+1] prefix sums of 8*(effective fanin+1) over the elements a sweep
+  // evaluates (gates that feed a gate or a PO)
+  std::vector<uint64_t> nfp_prefix;
+  std::vector<uint32_t> eval_prefix; // [N+1] prefix counts of those elements
   std::vector<uint32_t> level_off;   // [n_levels+1]
   std::vector<uint32_t> maxfo_level; // [N] highest non-PO consumer level (0 if none)
   std::vector<uint8_t> gate_fo;      // [N] has a non-PO consumer
@@ -144,11 +178,16 @@ struct CircuitPlan {
 struct Schedule {
   uint32_t G = 0;
   uint32_t max_live = 0;             // slots (multiple of G)
-  std::vector<SweepRec> recs;        // [N], positions of levels 1..max_gate_level used
+  std::vector<uint64_t> blob;        // level blocks (8-byte units; each block 16-byte aligned)
+  std::vector<LevelDesc> lvl;        // [n_levels+1]; levels 1..max_gate_level used
+  uint32_t max_block16 = 0;          // largest level block, 16-byte units
   std::vector<uint32_t> li_off;      // [n_levels+1]
   std::vector<uint32_t> li;          // pairs (element, slot)
   uint64_t conflict_groups = 0;      // group accesses whose slots repeat a residue
   uint64_t access_groups = 0;        // group accesses (fanin loads + stores)
+  uint64_t bytes() const {
+    return blob.size() * 8 + lvl.size() * sizeof(LevelDesc) + li_off.size() * 4 + li.size() * 4;
+  }
 };
 
 // 0: AND family (AND, NAND, OR, NOR, INV, CLKBUF, PO), 1: XOR family, 2: MUX.
@@ -162,8 +201,10 @@ void build_circuit_plan(const Netlist& nl, CircuitPlan& cplan);
 // members of the FFRs the faults touch).
 void build_fault_plan(const Netlist& nl, const CircuitPlan& cplan, const std::vector<Fault>& faults,
                       Plan& plan);
+// Class of a plain record, or kPlainClasses when the gate needs a wide one.
+uint32_t plain_class(uint8_t type, uint32_t eff_fanin);
 // G in {2, 4, 8, 16}.  A schedule that needs more than kMaxSlots slots
-// reports max_live > kMaxSlots and leaves li empty.
+// reports max_live > kMaxSlots and leaves blob and li empty.
 void build_schedule(const Netlist& nl, const Plan& plan, uint32_t G, Schedule& out);
 
 }  // namespace fsimb

@@ -60,6 +60,7 @@ struct ResidentCircuit {
   ClassShape shape{4, 256, 1};
   Patterns block;  // resident pattern block (host copy of its words)
   uint64_t block_tiles = 0;
+  // d_level_off holds the schedule's level descriptors, d_recs its record blocks
   DevBuf d_type, d_fi_off, d_fi_idx, d_level, d_level_off, d_recs, d_li_off, d_li, d_pwords, d_good;
   BatchCirc dev{};
   uint64_t device_bytes() const {
@@ -312,8 +313,8 @@ struct fsimb_server {
       upload(c->d_fi_off, nl.fi_off, s);
       upload(c->d_fi_idx, nl.fi_idx, s);
       upload(c->d_level, nl.level, s);
-      upload(c->d_level_off, B.level_off, s);
-      upload(c->d_recs, c->sched.recs, s);
+      upload(c->d_level_off, c->sched.lvl, s);
+      upload(c->d_recs, c->sched.blob, s);
       upload(c->d_li_off, c->sched.li_off, s);
       upload(c->d_li, c->sched.li, s);
       c->block_tiles = (c->block.W + kTileWords - 1) / kTileWords;
@@ -348,8 +349,8 @@ struct fsimb_server {
     c->dev.fi_off = c->d_fi_off.as<uint32_t>();
     c->dev.fi_idx = c->d_fi_idx.as<uint32_t>();
     c->dev.level = c->d_level.as<uint32_t>();
-    c->dev.level_off = c->d_level_off.as<uint32_t>();
-    c->dev.recs = c->d_recs.as<uint4>();
+    c->dev.lvl = c->d_level_off.as<uint4>();
+    c->dev.blob = c->d_recs.as<uint4>();
     c->dev.li_off = c->d_li_off.as<uint32_t>();
     c->dev.li = c->d_li.as<uint32_t>();
     std::lock_guard<std::mutex> g(circuits_mu);

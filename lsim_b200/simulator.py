@@ -152,10 +152,19 @@ class Simulator:
         self._check(_lib.lib().fsimb_set_patterns(self._h, _u64p(w), int(num_patterns)))
 
     # ------------------------------------------------------------ running
+    SWEEP_VARIANTS = {"auto": 0, "shared": 1, "global": 2}
+
     def run(self, mode=Mode.CUDA_B200, num_threads=1, drop=False, words_per_item=0,
-            block_threads=0, ctas_per_sm=0, tune=False, stream=None):
+            block_threads=0, ctas_per_sm=0, tune=False, stream=None, n_detect=0,
+            sweep_variant="auto", wait_test=False):
+        """Simulates every fault against every pattern on the GPU.  drop: stop
+        simulating a fault after the 2,048-pattern tile in which its count
+        reaches n_detect (1 when 0).  sweep_variant: where a sweep keeps its
+        live values ("auto", "shared" memory, "global" memory).  wait_test is
+        a test hook (see fsimb_opts.wait_test)."""
         o = _lib.Opts(ctypes.sizeof(_lib.Opts), 1 if drop else 0, words_per_item, block_threads,
-                      ctas_per_sm, 1 if tune else 0, stream)
+                      ctas_per_sm, 1 if tune else 0, stream, n_detect,
+                      self.SWEEP_VARIANTS[sweep_variant], 1 if wait_test else 0, 0)
         self._check(_lib.lib().fsimb_run(self._h, ctypes.byref(o)))
         self._ran = True
 

@@ -47,6 +47,27 @@ def test_no_alloc_matches_regular_entry_point():
             assert np.array_equal(out[k] & mask, ref), rd
 
 
+def test_no_alloc_second_circuit_after_a_larger_one():
+    """A smaller, different circuit called after a larger one through the same
+    static array: nothing of the first circuit's values may leak into it."""
+    big = gen.generate(n_gates=6000, n_pi=48, n_po=40, n_levels=30, n_patterns=2048, seed=93,
+                       faults="outputs")
+    small = gen.generate(n_gates=700, n_pi=20, n_po=15, n_levels=12, n_patterns=2048, seed=94,
+                         type_mask=gen.ALL_TYPES, faults="outputs")
+    sims = []
+    for w in (big, small):
+        s = Simulator(0)
+        s.read_text(w["ckt"], w["flst"], w["ptn"])
+        s.run()
+        sims.append(s)
+    for s in sims:
+        words = s.patterns()[:32]
+        out = _call(s, words, 32, s.num_POs())
+        first_po = s.num_PIs() + s.num_gates()
+        for rd in (0, 17, 31):
+            assert np.array_equal(out[rd], s.good_values(rd)[first_po:]), rd
+
+
 def test_no_alloc_rejects_out_of_range():
     w = gen.generate(n_gates=200, n_pi=8, n_po=6, n_levels=8, n_patterns=128, seed=5)
     sim = Simulator(0)
