@@ -51,27 +51,40 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "c2"
 METRIC = "fault×pattern evals/s (200k-gate)"
 UNIT = "fault-patterns/s"
+# The c2 workload's fixed sizes (seeded; checked against the loaded problem
+# in the GPU arm, so both arms print the same config).
+C2_FAULTS = 738943
+C2_PATTERNS = 65536
+C2_ELEMENTS = 202000
+# Shared-memory bandwidth of one SM: 32 banks x 4 bytes per clock.
+SMEM_BYTES_PER_CLK_SM = 128
 
 
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, "fallback (6.65 TB/s, an earlier copy measurement on this pool)"
 
 
-def _profile_traffic():
-    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_sweep_c2.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_per_launch_bytes:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+def _profile_summary():
+    """Per-launch DRAM bytes and on-chip counters of the sweep kernel from
+    the committed ncu summaries (key: value lines)."""
+    out = {}
+    for name in ("k_sweep_c2.md", "k_sweep_c2s.md"):
+        try:
+            for line in open(os.path.join(ROOT, "profiles", name)):
+                if ":" in line and line.split(":", 1)[0].strip().startswith(("traffic_", "ncu_")):
+                    k, v = line.split(":", 1)
+                    try:
+                        out[k.strip()] = float(v)
+                    except ValueError:
+                        pass
+        except OSError:
+            pass
+    return out
 
 
 class ClockSampler:
@@ -130,91 +143,151 @@ def _dist():
     return world, rank, local
 
 
-def _output_fault_sample(flst_text, n):
-    """First n output faults (pin 0) of an @pins list, as plain .flst text."""
-    toks = flst_text.split()
-    pins = toks[0] == "@pins"
-    if pins:
-        toks = toks[1:]
-    F = int(toks[0])
-    out = []
-    step = 3 if pins else 2
-    for i in range(F):
-        site, val = toks[1 + step * i], toks[2 + step * i]
-        pin = toks[3 + step * i] if pins else "0"
-        if pin == "0":
-            out.append("%s %s" % (site, val))
-            if len(out) == n:
-                break
-    return "%d\n%s\n" % (len(out), "\n".join(out))
+def _config(world, faults_sharded):
+    """The workload as both arms state it."""
+    patterns = C2_PATTERNS if (faults_sharded or world == 1) else world * C2_PATTERNS
+    return {"workload": "c2: 200,000 gates, 1,000 PI, 1,000 PO, 150 levels, mean fan-in 2.2; "
+                        "%d collapsed output+input-pin SA faults; 65,536 patterns%s"
+                        % (C2_FAULTS, "" if patterns == C2_PATTERNS else
+                           " per rank (%d ranks, own seed each)" % world),
+            "faults": C2_FAULTS, "patterns": patterns, "elements": C2_ELEMENTS, "mode": "count",
+            "parallelism": ("1 GPU" if world == 1 else
+                            "%s-sharded x%d" % ("fault" if faults_sharded else "pattern", world)),
+            "l2": "inputs larger than L2: the good-machine words (1.65 GB per 65,536-pattern "
+                  "block) are rewritten every step"}
 
 
-def cpu_baseline(w, target_s=15.0):
-    """The reference simulator (else the CPU port) on a bounded sample of the
-    workload: S output faults x R rounds, all faults sharded over threads."""
+def _ref_threads():
+    return max(1, min(64, os.cpu_count() or 1))
+
+
+def reference_sample(target_s=15.0, inputs=None):
+    """LSIM's own simulator (oracle/_ref; the CPU port in oracle/ when the
+    reference was not built) on a bounded sample of the c2 workload: its
+    first 4 x threads output faults (the reference's .flst cannot express
+    pin faults) over as many 64-pattern rounds as fit in about target_s,
+    faults sharded over all host threads.  Inputs come from the pure-Python
+    generator (tests/workload_py.py), so nothing of the product library is
+    loaded.  Returns (cpu_baseline dict, inputs)."""
     from tests.oracle_lib import Oracle, Reference, ref_available
-    threads = max(1, min(64, os.cpu_count() or 1))
-    full = Oracle(w["ckt"], "0\n", w["ptn"])
+    from tests import workload_py
+    threads = _ref_threads()
+    kind = "reference" if ref_available() else "port"
+    nf = 4 * threads if kind == "reference" else 32 * threads
+    if inputs is None or inputs["flst"].count("\n") - 1 < nf:
+        inputs = workload_py.c2_inputs(rounds=1024, n_output_faults=nf)
+    words, n_pi = inputs["words"], inputs["n_pi"]
+
+    def run(R):
+        w = words[:R]
+        if kind == "reference":
+            ref = Reference(inputs["ckt"], inputs["flst"], words=w, P=R * 64, n_pi=n_pi)
+            ref.simulate(threads=threads)
+            return ref.seconds, ref.F
+        o = Oracle(inputs["ckt"], inputs["flst"], "0\n")
+        o.set_patterns(w, R * 64)
+        t0 = time.perf_counter()
+        o.simulate(mode=0, threads=threads)
+        return time.perf_counter() - t0, len(o.faults)
+
+    per_round, _ = run(1)
+    R = int(max(1, min(len(words), target_s / max(per_round, 1e-3))))
+    secs, F = run(R)
+    value = F * R * 64 / secs
+    return ({"value": value, "unit": UNIT, "cores": threads, "kind": kind, "cpu": _cpu_model(),
+             "sample": "%d output faults x %d rounds (%d patterns) of the c2 workload, %.1f s, "
+                       "faults sharded over %d threads (full re-simulation per fault, "
+                       "fsim/simulation.cpp:104-147)" % (F, R, R * 64, secs, threads)}, inputs)
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def extra_cpu_baselines(c2_text=None):
+    """The reference's other CPU modes and the oracle's cone-limited
+    restatement, each on a bounded sample (a few seconds each)."""
+    from tests.oracle_lib import Oracle, Reference, ref_available
+    from tests import workload_py
+    out = []
+    threads = _ref_threads()
     if ref_available():
-        kind = "reference"
-        fl = _output_fault_sample(w["flst"], 4 * threads)
-        ref = Reference(w["ckt"], fl, words=full.words, P=full.P, n_pi=full.n_pi)
-        ref.simulate(rd0=0, rd1=1, threads=threads)          # load workers, calibrate
-        per_round = max(ref.seconds, 1e-3)
-        R = int(max(1, min(full.W, target_s / per_round)))
-        ref.simulate(rd0=0, rd1=R, threads=threads)
-        secs, nf = ref.seconds, ref.F
-    else:
-        kind = "port"
-        fl = _output_fault_sample(w["flst"], 32 * threads)
-        o = Oracle(w["ckt"], fl, w["ptn"])
+        c1 = dict(n_gates=2000, n_pi=64, n_po=64, n_levels=30, p_fanin3=0.5, seed=0)
+        ckt = workload_py.circuit(**c1)
+        words = workload_py.pattern_words(64, 4096, seed=0)
+        nf = 128
+        # SA0/SA1 on the first 64 gates by file id (c1's list is every gate output)
+        flst = "%d\n%s\n" % (nf, "\n".join("%d %d" % (128 + i // 2, i % 2) for i in range(nf)))
+        for mode, name, th in ((0, "SEQUENTIAL", 1), (2, "PARALLEL_OMP", threads),
+                               (1, "PARALLEL_TF", threads)):
+            ref = Reference(ckt, flst, words=words, P=4096, n_pi=64)
+            t0 = time.perf_counter()
+            ref.run_table(mode=mode, threads=th)
+            secs = time.perf_counter() - t0
+            out.append({"value": nf * 4096 / secs, "unit": UNIT, "cores": th, "kind": "reference",
+                        "mode": name, "cpu": _cpu_model(),
+                        "sample": "c1 (2,000 gates, 64 PI / 64 PO, 30 levels), %d output faults x "
+                                  "4,096 patterns through Simulator::run(%s, %d) "
+                                  "(fsim/simulation.cpp:65-92), %.2f s" % (nf, name, th, secs)})
+    if c2_text is not None:
+        # every 512th fault of the whole collapsed list (output and pin faults)
+        sel = np.arange(0, c2_text["n_faults"], 512)
+        fl = workload_py.flst_pins(c2_text["fault_fids"][sel], c2_text["fault_pins"][sel],
+                                   c2_text["fault_values"][sel])
+        R = min(64, len(c2_text["words"]))
+        o = Oracle(c2_text["ckt"], fl, "0\n")
+        o.set_patterns(c2_text["words"][:R], R * 64)
         t0 = time.perf_counter()
-        o.simulate(rd0=0, rd1=1, mode=0, threads=threads)
-        per_round = max(time.perf_counter() - t0, 1e-3)
-        R = int(max(1, min(full.W, target_s / per_round)))
-        t0 = time.perf_counter()
-        o.simulate(rd0=0, rd1=R, mode=0, threads=threads)
-        secs, nf = time.perf_counter() - t0, len(o.faults)
-    value = nf * R * 64 / secs
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": "%d output faults x %d rounds (%d patterns) of the %s workload, %.1f s"
-                      % (nf, R, R * 64, WORKLOAD, secs)}
+        o.simulate(mode=2, threads=threads)
+        secs = time.perf_counter() - t0
+        F = len(o.faults)
+        out.append({"value": F * R * 64 / secs, "unit": UNIT, "cores": threads, "kind": "port",
+                    "mode": "cone-limited restatement over chunks of rounds "
+                            "(oracle/fsim_oracle.c mode 2)",
+                    "cpu": _cpu_model(),
+                    "sample": "c2, every 512th fault of the collapsed list (%d output and pin "
+                              "faults) x %d rounds, %.2f s" % (F, R, secs)})
+    return out
 
 
 def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
         return
-    from lsim_b200 import gen
-    w = gen.workload(WORKLOAD)
-    n_faults = int(w["flst"].split()[1 if w["flst"].startswith("@pins") else 0])
+    faults_sharded = args.shard == "faults"
+    cfg = _config(world, faults_sharded)
+    units = C2_FAULTS * cfg["patterns"]
+    # each step a bounded sample sized so that the whole run takes a few minutes
+    per_step = max(2.0, min(args.ref_seconds, 150.0 / max(1, args.steps + args.warmup)))
+    inputs = None
     for _ in range(args.warmup):
-        cpu_baseline(w, target_s=2.0)
-    vals, secs = [], []
+        _, inputs = reference_sample(target_s=min(2.0, per_step), inputs=inputs)
+    vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        b = cpu_baseline(w, target_s=args.ref_seconds)
+        b, inputs = reference_sample(target_s=per_step, inputs=inputs)
         vals.append(b["value"])
     elapsed = time.perf_counter() - t0
     value = statistics.median(vals)
-    P = 65536
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * n_faults * P / value,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": _workload_desc(n_faults), "mode": "count",
-                       "timed": "bounded sample per step; ms_per_step extrapolated to the full job"},
+            "ms_per_step": 1000.0 * units / value,
+            "higher_is_better": True, "scaling": "strong" if faults_sharded else "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+            "config": cfg,
+            "timed": "each step is a bounded sample of the workload (output faults x rounds, "
+                     "see cpu_baseline.sample); ms_per_step is the full job at the sample's rate",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": b["cores"], "kind": b["kind"],
-                             "sample": b["sample"]},
+                             "cpu": b["cpu"], "sample": b["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": elapsed}
     print(json.dumps(line), flush=True)
-
-
-def _workload_desc(n_faults):
-    return ("c2: 200,000 gates, 1,000 PI, 1,000 PO, 150 levels, mean fan-in 2.2; %d collapsed "
-            "output+input-pin SA faults; 65,536 patterns" % n_faults)
 
 
 def run_ours(args):
@@ -236,6 +309,9 @@ def run_ours(args):
     sim = Simulator(local)
     sim.read_text(w["ckt"], w["flst"], w["ptn"])
     F_all = sim.info().num_faults
+    if F_all != C2_FAULTS or sim.info().num_elements != C2_ELEMENTS:
+        raise RuntimeError("the c2 workload changed: %d faults, %d elements"
+                           % (F_all, sim.info().num_elements))
     my_faults = None
     if faults_sharded and world > 1:
         site, pin, val = sim.faults()
@@ -252,10 +328,13 @@ def run_ours(args):
     def merge(res):
         if world == 1:
             return res
+        # rank 0 reports: the parts are gathered (fault shards) or reduced
+        # (pattern shards) onto it only
         if faults_sharded:
-            return shard.merge_fault_shards(res, my_faults, F_all, info.num_rounds, device="cuda")
+            return shard.merge_fault_shards(res, my_faults, F_all, info.num_rounds, device="cuda",
+                                            dst=0)
         return shard.merge_results(res, rank * P, rank == world - 1, world * info.num_rounds,
-                                   device="cuda")
+                                   device="cuda", dst=0)
 
     tune_ms = 0.0
     for _ in range(args.warmup):
@@ -272,7 +351,7 @@ def run_ours(args):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    sweep_ms, sweep_bytes, tiles, launches = 0.0, 0, 0, 0
+    sweep_ms, sweep_bytes, tiles, launches, gwe, good_gwe = 0.0, 0, 0, 0, 0, 0
     for _ in range(args.steps):
         sim.run(stream=sp, tune=True)
         merged = merge(sim.results())
@@ -281,6 +360,8 @@ def run_ours(args):
         sweep_bytes += st["sweep_alg_bytes"]
         tiles += st["n_tiles"]
         launches += st["kernel_launches"]
+        gwe += st["dense_gate_words"]
+        good_gwe += st["good_gate_words"]
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -314,59 +395,107 @@ def run_ours(args):
     units = (float(F_all) if faults_sharded else float(world) * F) * P * args.steps
     value = units / (ms / 1e3)
     e2e = units / (ms_e2e / 1e3)
-    peak, peak_src = _peaks()
-    per_launch_bytes = sweep_bytes / max(1, tiles)
-    per_launch_s = sweep_ms / max(1, tiles) / 1e3
-    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     st = sim.stats()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "strong" if faults_sharded else "weak", "vs_baseline": None, "dtype": "u64",
-        "data": "synthetic",
-        "config": {"workload": _workload_desc(F_all), "faults": F_all, "patterns": P,
-                   "elements": info.num_elements, "mode": "count",
-                   "parallelism": ("1 GPU" if world == 1 else
-                                   "%s-sharded x%d" % ("fault" if faults_sharded else "pattern", world)),
-                   "l2": "inputs larger than L2: good-machine words %.2f GB rewritten each step"
-                         % (info.num_elements * info.num_rounds * 8 / 1e9),
-                   "sweep": {"words_per_item": st["words_per_item"],
-                             "block_threads": st["block_threads"], "blocks": st["blocks"],
-                             "ctas_per_sm": st["ctas_per_sm"], "smem_bytes": st["smem_bytes"],
-                             "max_live": st["max_live"],
-                             "shape": "autotuned during warm-up on a strided sample of the "
-                                      "first tile's sweeps", "tune_ms": tune_ms}},
+        "data": "synthetic", "config": _config(world, faults_sharded),
         "e2e": {"value": e2e, "unit": UNIT,
                 "h2d_bytes_per_step": int(words.nbytes),
                 "d2h_bytes_per_step": int(F * 17)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": _profile_traffic(),
-                     "kernel": "k_sweep", "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
-                     "per_launch_alg_bytes": per_launch_bytes, "per_launch_ms": per_launch_s * 1e3},
+        "gate_word_evals_per_s": {
+            "sweep_dense": gwe / (ms / 1e3) * (world if not faults_sharded else 1),
+            "good_machine": good_gwe / (ms / 1e3) * (world if not faults_sharded else 1),
+            "per_step_sweep": gwe / args.steps,
+            "definition": "one gate evaluated on one 64-pattern word; the sweeps evaluate every "
+                          "gate above the flipped element's level (dense), per sweep and word"},
+        "sweep": {"words_per_item": st["words_per_item"], "block_threads": st["block_threads"],
+                  "blocks": st["blocks"], "ctas_per_sm": st["ctas_per_sm"],
+                  "smem_bytes": st["smem_bytes"], "max_live": st["max_live"],
+                  "shape": "autotuned during warm-up on a strided sample of the first tile's "
+                           "sweeps", "tune_ms": tune_ms},
         "breakdown_ms_per_step": {"good": st["ms_good"], "sweep": st["ms_sweep"],
                                   "ffr": st["ms_ffr"], "compute": st["ms_compute"],
                                   "total": st["ms_total"]},
         "clocks": clk,
     }
+    line.update(_rooflines(sweep_ms / max(1, tiles) / 1e3, sweep_bytes / max(1, tiles),
+                           st, clk))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, target_s=args.ref_seconds)
+        b, inputs = reference_sample(target_s=args.ref_seconds)
+        line["cpu_baseline"] = b
+        line["cpu_baselines_other"] = extra_cpu_baselines(inputs)
+    sim.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["batched"] = batch_summary(args.extra_circuits, steps=2)
+        line["served"] = serve_summary(n_req=args.requests, rates=[1.0])
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
+def _rooflines(launch_s, alg_bytes, st, clk):
+    """HBM roofline of the sweep kernel from its compulsory DRAM bytes, and
+    the on-chip roofline that binds it (shared-memory bandwidth)."""
+    peak, peak_src = _peaks()
+    prof = _profile_summary()
+    traffic = prof.get("traffic_per_launch_bytes")
+    # compulsory DRAM bytes of one launch: the tile's good words, the gate
+    # records and live-in lists of the schedule, the sweep output rows
+    compulsory = st["hbm_bytes_per_tile"]
+    hbm = compulsory / launch_s / 1e9 if launch_s > 0 else 0.0
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    smem_peak = SMEM_BYTES_PER_CLK_SM * 148 * mhz * 1e6 / 1e9
+    onchip = alg_bytes / launch_s / 1e9 if launch_s > 0 else 0.0
+    return {
+        "roofline": {"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s",
+                     "frac": hbm / peak, "traffic": traffic, "kernel": "k_sweep",
+                     "peak_source": peak_src,
+                     "per_launch_bytes": compulsory, "per_launch_ms": launch_s * 1e3,
+                     "note": "achieved = compulsory DRAM bytes of one launch (good words of the "
+                             "tile, gate records, live-in lists, output rows) / its CUDA-event "
+                             "time; traffic = ncu dram bytes of one launch. Values stay in "
+                             "shared memory, so HBM is not what binds this kernel (see onchip)"},
+        "onchip": {"bound": "shared-memory bandwidth", "achieved": onchip, "peak": smem_peak,
+                   "unit": "GB/s", "frac": onchip / smem_peak,
+                   "peak_source": "architectural: 128 B/clock/SM x 148 SMs x the median SM clock "
+                                  "sampled during the timed region (%.0f MHz)" % mhz,
+                   "per_launch_alg_bytes": alg_bytes,
+                   "achieved_definition": "8*(fanin+1) bytes per gate-word evaluation: the "
+                                          "fanin words read and the output word written, all "
+                                          "in shared memory",
+                   "ncu": {k[4:]: v for k, v in prof.items() if k.startswith("ncu_")}},
+    }
+
+
 def run_batch(args):
     """Batched configuration: one batch of 256 circuits against 256 plain runs."""
+    print(json.dumps(batch_measure(args.circuits, args.steps, args.warmup)), flush=True)
+
+
+def batch_summary(n_circuits, steps=2):
+    """The batched configuration's figures for the default bench line."""
+    m = batch_measure(n_circuits, steps, warmup=1, full=False)
+    return {"workload": m["config"]["workload"], "steps": steps, "value": m["value"],
+            "unit": UNIT, "ms_per_step": m["ms_per_step"], "plain_sequential": m["plain_sequential"],
+            "batch_over_plain": m["batch_over_plain"], "e2e": m["e2e"],
+            "plain_sequential_e2e": m["plain_sequential_e2e"], "gpu_launches": m["gpu_launches"],
+            "n_classes": m["config"]["sweep"]["n_classes"], "graph": m["config"]["graph"],
+            "tune_ms": m["config"]["tune_ms"], "results_equal_plain": m["results_equal_plain"],
+            "clocks": m["clocks"]}
+
+
+def batch_measure(n_circuits, steps, warmup, full=True):
     import torch
     from lsim_b200 import Batch, Simulator, gen
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    cfgs = gen.batch_configs(args.circuits, seed=0)
+    cfgs = gen.batch_configs(n_circuits, seed=0)
     t0 = time.perf_counter()
     ws = [gen.generate(**c) for c in cfgs]
     gen_s = time.perf_counter() - t0
@@ -400,20 +529,20 @@ def run_batch(args):
     b.run(tune=True, stream=sp)
     first_s = time.perf_counter() - t0
     tune_ms = b.stats()["ms_tune"]
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         b.run(tune=True, stream=sp)
     for p in plains:
         p.run(stream=sp, tune=True)
     clocks = ClockSampler(0)
     clocks.start()
-    ms_batch = timed(lambda: b.run(tune=True, stream=sp), args.steps)
+    ms_batch = timed(lambda: b.run(tune=True, stream=sp), steps)
     st = b.stats()
-    ms_serial = timed(lambda: b.run(tune=True, concurrent=False, stream=sp), args.steps)
-    ms_plain = timed(lambda: [p.run(stream=sp, tune=True) for p in plains], args.steps)
+    ms_serial = timed(lambda: b.run(tune=True, concurrent=False, stream=sp), steps) if full else None
+    ms_plain = timed(lambda: [p.run(stream=sp, tune=True) for p in plains], steps)
     clk = clocks.stop()
     plain_launches = sum(p.stats()["kernel_launches"] for p in plains)
     # e2e: every input from host memory each step
-    ms_batch_e2e = timed(lambda: b.run(tune=True, reupload=True, stream=sp), args.steps)
+    ms_batch_e2e = timed(lambda: b.run(tune=True, reupload=True, stream=sp), steps)
     st_e2e = b.stats()
     words = [p.patterns() for p in plains]
     pinned = [torch.from_numpy(wd.ravel()).pin_memory().numpy() for wd in words]
@@ -423,70 +552,83 @@ def run_batch(args):
             p.set_patterns(wd, m.info().num_patterns)
             p.run(stream=sp, tune=True)
             p.results()
-    ms_plain_e2e = timed(plain_e2e, args.steps)
-    # phase split of one step of each arm (batch without the graph)
-    b.run(tune=True, graph=False, stream=sp)
-    st_ng = b.stats()
-    classes = b.classes()
-    phases = {"batch": {k: st_ng[k] for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")},
-              "plain": {k: sum(p.stats()[k] for p in plains)
-                        for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")}}
+    ms_plain_e2e = timed(plain_e2e, steps)
+    phases, classes = None, None
+    if full:
+        # phase split of one step of each arm (batch without the graph)
+        b.run(tune=True, graph=False, stream=sp)
+        st_ng = b.stats()
+        classes = b.classes()
+        phases = {"batch": {k: st_ng[k] for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")},
+                  "plain": {k: sum(p.stats()[k] for p in plains)
+                            for k in ("ms_good", "ms_sweep", "ms_ffr", "ms_total")}}
     # results agree with the plain path on every circuit
     same = all(np.array_equal(m.results(), p.results()) for m, p in zip(members, plains))
-    peak, peak_src = _peaks()
-    sweep_s = st["ms_compute"] / 1e3
     line = {
-        "metric": "fault×pattern evals/s (batched, %d circuits)" % args.circuits,
-        "value": FP * args.steps / (ms_batch / 1e3), "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+        "metric": "fault×pattern evals/s (batched, %d circuits)" % n_circuits,
+        "value": FP * steps / (ms_batch / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": steps, "warmup": warmup, "ms_per_step": ms_batch / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic",
         "config": {"workload": "c4: %d circuits, %d-%d gates (median %d), 10-120 levels, SA0/SA1 "
                                "on every gate output (%d faults), 1,024-16,384 patterns"
-                               % (args.circuits, min(gates), max(gates), int(np.median(gates)), F),
+                               % (n_circuits, min(gates), max(gates), int(np.median(gates)), F),
                    "fault_patterns_per_step": FP, "mode": "count",
                    "sweep": {k: st[k] for k in ("words_per_item", "block_threads", "ctas_per_sm",
                                                 "blocks", "smem_bytes", "n_classes")},
                    "graph": bool(st["graph_used"]), "tune_ms": tune_ms,
                    "first_run_s": first_s, "generate_s": gen_s},
-        "plain_sequential": {"value": FP * args.steps / (ms_plain / 1e3),
-                             "ms_per_step": ms_plain / args.steps,
+        "plain_sequential": {"value": FP * steps / (ms_plain / 1e3),
+                             "ms_per_step": ms_plain / steps,
                              "gpu_launches_per_step": int(plain_launches)},
         "batch_over_plain": ms_plain / ms_batch,
-        "batch_serial_classes": {"value": FP * args.steps / (ms_serial / 1e3),
-                                 "ms_per_step": ms_serial / args.steps},
-        "e2e": {"value": FP * args.steps / (ms_batch_e2e / 1e3), "unit": UNIT,
+        "e2e": {"value": FP * steps / (ms_batch_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": int(st_e2e["h2d_bytes"]),
                 "d2h_bytes_per_step": int(st_e2e["d2h_bytes"])},
-        "plain_sequential_e2e": {"value": FP * args.steps / (ms_plain_e2e / 1e3),
-                                 "ms_per_step": ms_plain_e2e / args.steps},
-        "gpu_launches": int(st["kernel_launches"]) * args.steps,
+        "plain_sequential_e2e": {"value": FP * steps / (ms_plain_e2e / 1e3),
+                                 "ms_per_step": ms_plain_e2e / steps},
+        "gpu_launches": int(st["kernel_launches"]) * steps,
         "breakdown_ms_per_step": {"compute": st["ms_compute"], "d2h": st["ms_d2h"],
                                   "total": st["ms_total"]},
-        "roofline": {"bound": "hbm", "achieved": st["sweep_alg_bytes"] / sweep_s / 1e9,
-                     "peak": peak, "unit": "GB/s",
-                     "frac": st["sweep_alg_bytes"] / sweep_s / 1e9 / peak, "traffic": None,
-                     "kernel": "whole batch (good + sweeps + tracing)",
-                     "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)"},
-        "phases_ms_per_step": phases,
-        "classes": classes,
+        "gate_word_evals_per_s": {"sweep_dense": st["dense_gate_words"] / (ms_batch / steps / 1e3)},
         "results_equal_plain": same,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    if full:
+        line["batch_serial_classes"] = {"value": FP * steps / (ms_serial / 1e3),
+                                        "ms_per_step": ms_serial / steps}
+        line["phases_ms_per_step"] = phases
+        line["classes"] = classes
     b.close()
+    for m in members + plains:
+        m.close()
+    return line
 
 
 def run_serve(args):
     """Serving configuration: requests against 32 resident circuits, served
     by the server (waves on concurrent slots) and by the plain path one job
     at a time, at a burst and at Poisson arrival rates."""
+    n_circ = args.circuits if args.circuits != 256 else 32
+    print(json.dumps(serve_measure(n_circ, args.requests, args.rates, args.slots, args.slot_gib)),
+          flush=True)
+
+
+def serve_summary(n_req=200, rates=(1.0,), n_circuits=32):
+    """The serving configuration's figures for the default bench line."""
+    m = serve_measure(n_circuits, n_req, list(rates), 2, 8)
+    return {"workload": m["config"]["workload"], "unit": UNIT, "burst": m["burst"],
+            "poisson": m["poisson"], "rates": m["config"]["rates"],
+            "results_equal_plain": m["results_equal_plain"], "clocks": m["clocks"]}
+
+
+def serve_measure(n_circuits, n_req, rates, slots, slot_gib):
     import threading
     import torch
     from lsim_b200 import Server, Simulator, gen
     torch.cuda.set_device(0)
     rng = np.random.default_rng(0)
-    cfgs = gen.serve_configs(args.circuits if args.circuits != 256 else 32, seed=0)
+    cfgs = gen.serve_configs(n_circuits, seed=0)
     block_P = 16384
     circs = []
     t0 = time.perf_counter()
@@ -503,7 +645,6 @@ def run_serve(args):
     gen_s = time.perf_counter() - t0
     # the request stream: circuit, fault subset (1,000-100,000, log-uniform,
     # at most the circuit's list), 64-8,192 patterns from a tile-aligned window
-    n_req = args.requests
     reqs = []
     for _ in range(n_req):
         ci = int(rng.integers(len(circs)))
@@ -518,7 +659,7 @@ def run_serve(args):
                          value=c["value"][idx].copy(), P=P, row0=row0))
     FP = sum(len(r["site"]) * r["P"] for r in reqs)
 
-    srv = Server(0, slots=args.slots, slot_bytes=args.slot_gib << 30)
+    srv = Server(0, slots=slots, slot_bytes=slot_gib << 30)
     t0 = time.perf_counter()
     ids = [srv.add_circuit(c["ckt"], c["words"], block_P) for c in circs]
     add_s = time.perf_counter() - t0
@@ -584,7 +725,7 @@ def run_serve(args):
     burst_plain = plain_at(None)
     cap = n_req / (FP / burst_plain["value"])  # plain path capacity, requests/s
     rows = []
-    for f in args.rates:
+    for f in rates:
         rows.append({"load": f, "server": serve_at(f * cap), "plain": plain_at(f * cap)})
     clk = clocks.stop()
     # results of the mix equal the plain path's, request by request
@@ -611,7 +752,7 @@ def run_serve(args):
                                "resident blocks; %d requests of 1,000-100,000 faults and 64-8,192 "
                                "patterns" % (len(circs), min(gates), max(gates),
                                              int(np.median(gates)), block_P, n_req),
-                   "fault_patterns": FP, "slots": args.slots, "slot_gib": args.slot_gib,
+                   "fault_patterns": FP, "slots": slots, "slot_gib": slot_gib,
                    "generate_s": gen_s, "add_circuits_s": add_s,
                    "resident_bytes": st["resident_bytes"], "slot_bytes": st["slot_bytes"],
                    "rates": "fractions of the plain path's burst capacity (%.2f requests/s)" % cap},
@@ -620,8 +761,10 @@ def run_serve(args):
         "results_equal_plain": same,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
     srv.close()
+    for p in plains:
+        p.close()
+    return line
 
 
 def main():
@@ -632,6 +775,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave the batched (c4) and served (c5) summaries out of the c2 line")
+    ap.add_argument("--extra-circuits", type=int, default=256,
+                    help="circuits of the batched summary in the c2 line")
     ap.add_argument("--workload", default=WORKLOAD, help="c2 (default) or another gen.WORKLOADS key")
     ap.add_argument("--shard", default="patterns", choices=["patterns", "faults"],
                     help="with --gpus N > 1: each rank its own pattern block (weak scaling, "
