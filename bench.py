@@ -818,9 +818,18 @@ def main():
         return
     if args.profile:
         from lsim_b200 import Simulator, gen
-        w = gen.workload(args.workload)
+        if args.workload == "c3":
+            # the stated stress list: the collapsed output + input-pin faults of
+            # the 2M-gate circuit, 4,000,000 of them drawn with seed 0
+            w = gen.workload("c3", faults="collapsed")
+        else:
+            w = gen.workload(args.workload)
         sim = Simulator(0)
         sim.read_text(w["ckt"], w["flst"], w["ptn"])
+        if args.workload == "c3":
+            site, pin, val = sim.faults()
+            keep = np.sort(np.random.default_rng(0).choice(len(site), size=4000000, replace=False))
+            sim.set_faults(site[keep], pin[keep], val[keep])
         shape = {}
         if args.shape:
             M, T, occ = (int(x) for x in args.shape.split(","))
@@ -833,9 +842,12 @@ def main():
         res = sim.results()
         info = sim.info()
         print(json.dumps({"workload": args.workload, "faults": info.num_faults,
+                          "pin_faults": int((sim.faults()[1] > 0).sum()),
                           "patterns": info.num_patterns, "elements": info.num_elements,
                           "mode": "drop" if args.drop else "count", "wall_s": wall,
-                          "detected": int(res["detected"].sum()), "stats": st}))
+                          "detected": int(res["detected"].sum()),
+                          "gate_word_evals_per_s": st["dense_gate_words"] / max(st["ms_sweep"], 1e-9) * 1e3,
+                          "stats": st}))
         return
     if args.impl == "reference":
         run_reference(args)

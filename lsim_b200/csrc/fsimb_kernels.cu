@@ -211,25 +211,7 @@ __device__ __forceinline__ void sts_chunk(uint64_t* vals, uint32_t slot, int h, 
 template <int M>
 using PoAcc = uint64_t[(M >= 2) ? M / 2 : 1][(M >= 2) ? 2 : 1];
 
-// ---- plain records: one compile-time body per gate class
-template <uint32_t CLS>
-__device__ __forceinline__ uint64_t plain_fn(uint64_t a, uint64_t b, uint64_t c) {
-  if constexpr (CLS == kPBuf) return a;
-  else if constexpr (CLS == kPInv) return ~a;
-  else if constexpr (CLS == kPAnd2) return a & b;
-  else if constexpr (CLS == kPNand2) return ~(a & b);
-  else if constexpr (CLS == kPOr2) return a | b;
-  else if constexpr (CLS == kPNor2) return ~(a | b);
-  else if constexpr (CLS == kPXor2) return a ^ b;
-  else if constexpr (CLS == kPXnor2) return ~(a ^ b);
-  else if constexpr (CLS == kPAnd3) return a & b & c;
-  else if constexpr (CLS == kPNand3) return ~(a & b & c);
-  else if constexpr (CLS == kPOr3) return a | b | c;
-  else if constexpr (CLS == kPNor3) return ~(a | b | c);
-  else if constexpr (CLS == kPXor3) return a ^ b ^ c;
-  else return ~(a ^ b ^ c);
-}
-
+// ---- plain records: one body per family and fan-in (fsimb_plan.h plain_body)
 // Slot chunk h of the value at byte offset `off` (slot * 8M).
 template <int M>
 __device__ __forceinline__ void ldo(const char* vb, uint32_t off, int h, uint64_t (&v)[2]) {
@@ -249,13 +231,28 @@ __device__ __forceinline__ void sto(char* vb, uint32_t off, int h, const uint64_
     *reinterpret_cast<ulonglong2*>(vb + off + 16 * h) = make_ulonglong2(v[0], v[1]);
 }
 
-// A plain record (fsimb_plan.h plain_rec) of class CLS on all M words.
-template <int M, uint32_t CLS>
+// A plain record (fsimb_plan.h plain_rec) of body B on all M words.  B = 0:
+// one input, io ^ a; 1 / 3: AND family with 2 / 3 inputs,
+// io ^ AND(in ^ ii); 2 / 4: XOR family with 2 / 3 inputs, io ^ XOR(in).
+// The inversions come from the class code: within the AND family the codes
+// run AND, NAND, OR, NOR, so ii is bit 1 of the offset and io the XOR of
+// its two bits; elsewhere io is bit 0 of the code.
+template <int M, int B>
 __device__ __forceinline__ void plain_body(char* vb, const uint2 r, int pl) {
   constexpr int C = (M >= 2) ? M / 2 : 1;
   constexpr int VC = (M >= 2) ? 2 : 1;
-  constexpr int NF = CLS <= kPInv ? 1 : (CLS <= kPXnor2 ? 2 : 3);
+  constexpr int NF = B == 0 ? 1 : (B <= 2 ? 2 : 3);
   constexpr uint32_t SB = 8u * M;
+  const uint32_t cls = r.y >> 28;
+  uint32_t io_bit, ii_bit = 0;
+  if constexpr (B == 1 || B == 3) {
+    const uint32_t rel = cls - (B == 1 ? (uint32_t)kPAnd2 : (uint32_t)kPAnd3);
+    ii_bit = (rel >> 1) & 1u;
+    io_bit = (rel ^ (rel >> 1)) & 1u;
+  } else {
+    io_bit = cls & 1u;
+  }
+  const uint64_t ii = 0ull - (uint64_t)ii_bit, io = 0ull - (uint64_t)io_bit;
   const uint32_t o0 = (r.x & 0x7FFFu) * SB;
   const uint32_t o1 = ((r.x >> 15) & 0x7FFFu) * SB;
   const uint32_t o2 = (__funnelshift_r(r.x, r.y, 30) & 0x7FFFu) * SB;
@@ -268,28 +265,30 @@ __device__ __forceinline__ void plain_body(char* vb, const uint2 r, int pl) {
     if constexpr (NF > 1) ldo<M>(vb, o1, h, b);
     if constexpr (NF > 2) ldo<M>(vb, o2, h, d);
 #pragma unroll
-    for (int v = 0; v < VC; ++v) o[v] = plain_fn<CLS>(a[v], b[v], d[v]);
+    for (int v = 0; v < VC; ++v) {
+      if constexpr (B == 0)
+        o[v] = a[v] ^ io;
+      else if constexpr (B == 1)
+        o[v] = ((a[v] ^ ii) & (b[v] ^ ii)) ^ io;
+      else if constexpr (B == 2)
+        o[v] = a[v] ^ b[v] ^ io;
+      else if constexpr (B == 3)
+        o[v] = ((a[v] ^ ii) & (b[v] ^ ii) & (d[v] ^ ii)) ^ io;
+      else
+        o[v] = a[v] ^ b[v] ^ d[v] ^ io;
+    }
     sto<M>(vb, oo, h, o);
   }
 }
 
 template <int M>
 __device__ __forceinline__ void plain_dispatch(char* vb, const uint2 r, int pl) {
-  switch (r.y >> 28) {  // class, sorted on the host so a warp mostly takes one case
-    case kPBuf: plain_body<M, kPBuf>(vb, r, pl); break;
-    case kPInv: plain_body<M, kPInv>(vb, r, pl); break;
-    case kPAnd2: plain_body<M, kPAnd2>(vb, r, pl); break;
-    case kPNand2: plain_body<M, kPNand2>(vb, r, pl); break;
-    case kPOr2: plain_body<M, kPOr2>(vb, r, pl); break;
-    case kPNor2: plain_body<M, kPNor2>(vb, r, pl); break;
-    case kPXor2: plain_body<M, kPXor2>(vb, r, pl); break;
-    case kPXnor2: plain_body<M, kPXnor2>(vb, r, pl); break;
-    case kPAnd3: plain_body<M, kPAnd3>(vb, r, pl); break;
-    case kPNand3: plain_body<M, kPNand3>(vb, r, pl); break;
-    case kPOr3: plain_body<M, kPOr3>(vb, r, pl); break;
-    case kPNor3: plain_body<M, kPNor3>(vb, r, pl); break;
-    case kPXor3: plain_body<M, kPXor3>(vb, r, pl); break;
-    case kPXnor3: plain_body<M, kPXnor3>(vb, r, pl); break;
+  switch (r.y >> 28) {  // records are grouped by body on the host, so a warp mostly takes one case
+    case kPBuf: case kPInv: plain_body<M, 0>(vb, r, pl); break;
+    case kPAnd2: case kPNand2: case kPOr2: case kPNor2: plain_body<M, 1>(vb, r, pl); break;
+    case kPXor2: case kPXnor2: plain_body<M, 2>(vb, r, pl); break;
+    case kPAnd3: case kPNand3: case kPOr3: case kPNor3: plain_body<M, 3>(vb, r, pl); break;
+    case kPXor3: case kPXnor3: plain_body<M, 4>(vb, r, pl); break;
     default: break;  // kPNop
   }
 }

@@ -426,7 +426,7 @@ void build_schedule(const Netlist& nl, const Plan& P, uint32_t G, Schedule& S) {
       std::stable_sort(leftover.begin(), leftover.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
       make_groups(leftover, true);
     };
-    part(plain, [&](uint32_t e) { return plain_class(nl.type[e], nf_of(e)); });
+    part(plain, [&](uint32_t e) { return plain_body(plain_class(nl.type[e], nf_of(e))); });
     uint32_t n_plain = (uint32_t)order.size();
     // the wide part starts on a group boundary: pad with no-op records
     const uint32_t n_pad = wide.empty() ? 0 : (G - n_plain % G) % G;

@@ -55,6 +55,15 @@ enum PlainClass : uint32_t {
   kPBuf = 0, kPInv, kPAnd2, kPNand2, kPOr2, kPNor2, kPXor2, kPXnor2,
   kPAnd3, kPNand3, kPOr3, kPNor3, kPXor3, kPXnor3, kPlainClasses, kPNop = 15
 };
+// Classes that share one sweep body, which reads the class's input and
+// output inversions from the class code at run time: one input, AND family
+// (AND, NAND, OR, NOR) with two and with three inputs, XOR family with two
+// and with three inputs.  The host groups records by body, not by class:
+// larger groups leave fewer repeated bank residues and fewer class
+// boundaries inside a warp.
+inline uint32_t plain_body(uint32_t cls) {
+  return cls < kPAnd2 ? 0u : cls < kPXor2 ? 1u : cls < kPAnd3 ? 2u : cls < kPXor3 ? 3u : 4u;
+}
 // Bits [0,15) fanin 0, [15,30) fanin 1, [30,45) fanin 2, [45,60) output
 // slot, [60,64) class.
 inline uint64_t plain_rec(uint32_t f0, uint32_t f1, uint32_t f2, uint32_t out, uint32_t cls) {
