@@ -356,9 +356,9 @@ void fsimb_handle::run(const fsimb_opts* opts) {
   if (!wide && o.sweep_variant == 0 && n_sweeps &&
       (plan.max_live > kMaxSlots || sweep_vals_bytes(plan.max_live, 1) > share1))
     wide = true;  // no schedule can fit: skip building them
+  const bool explicit_shape = o.words_per_item || o.block_threads || o.ctas_per_sm;
   if (!wide && n_sweeps) {
     try {
-      const bool explicit_shape = o.words_per_item || o.block_threads || o.ctas_per_sm;
       if (explicit_shape) {
         M = (int)o.words_per_item;
         occ = o.ctas_per_sm ? (int)o.ctas_per_sm : 1;
@@ -400,13 +400,15 @@ void fsimb_handle::run(const fsimb_opts* opts) {
       if (!threads) threads = (int)pick_sweep_threads(widths, M);
       threads = std::min<int>(threads, (int)sweep_max_threads(M));
     } catch (const LimitError&) {
-      if (o.sweep_variant == 1) throw;
+      // an explicit shape that does not fit stays an error; without one, the
+      // circuit does not fit shared memory at any shape
+      if (o.sweep_variant == 1 || explicit_shape) throw;
       wide = true;
     }
   }
   int blocks = 0, occ_got = 0;
   if (wide) {
-    M = o.words_per_item ? (int)o.words_per_item : 2;
+    M = o.words_per_item == 1 ? 1 : 2;
     threads = 256;
     if (!eflag_uploaded) {
       std::vector<uint8_t> fl(N, 0);
