@@ -19,7 +19,17 @@ with --shard faults each rank simulates its part of the fault list (whole
 fanout-free-region groups, balanced by estimated cost) over the same
 patterns, merged the same way (strong scaling).
 --impl reference times LSIM's own CPU simulator (oracle/_ref, else the CPU
-port in oracle/) on a bounded sample of the same workload on all host cores.
+port in oracle/) on a bounded sample of the same workload on all host cores;
+its inputs come from the pure-Python generator (tests/workload_py.py), so
+that process loads no library of this package.  Both arms print the same
+config.
+
+The default line also carries: gate-word evaluations per second; an HBM
+roofline (compulsory DRAM bytes of a sweep launch over its time) and the
+on-chip one that binds the sweep (operand bytes through shared memory);
+the reference's other CPU modes and the oracle's cone-limited restatement
+(cpu_baselines_other); and, at N = 1, the batched (c4, 2 steps) and served
+(c5, burst and one Poisson rate) summaries (--no-extras leaves them out).
 
 --workload c4 times the batched configuration instead: 256 circuits
 (gen.batch_configs: 500-50,000 gates log-uniform, 10-120 levels, SA0/SA1 on
