@@ -9,12 +9,16 @@
 //                  (slots and a bank-conflict-free order chosen on the host;
 //                  gate records staged per level by TMA bulk copies).  Writes
 //                  the OR over POs of (faulty ^ good) per word.
+//   k_sweep_wide<M> the same sweep for circuits whose live values do not
+//                  fit in shared memory: values in a per-CTA region of global
+//                  memory indexed by element.
 //   k_ffr          one warp per FFR root, lanes = the 32 words of a tile:
 //                  backward critical-path tracing inside the FFR and the
 //                  per-fault detection word, count and first pattern.
 //   k_exact        the same epilogue for faults simulated by an exact sweep.
 //   k_drop         fault dropping: warp-aggregated stream compaction of the
-//                  roots / sweeps that still carry undetected faults.
+//                  roots / sweeps that still carry faults below the N-detect
+//                  limit.
 //
 // Word semantics follow fsim/simulation.cpp: gates act on whole 64-bit words
 // (fsim/simulation.cpp:979-1124), the last round keeps its high bits until
