@@ -287,13 +287,23 @@ __device__ __forceinline__ void plain_body(char* vb, const uint2 r, int pl) {
 
 template <int M>
 __device__ __forceinline__ void plain_dispatch(char* vb, const uint2 r, int pl) {
-  switch (r.y >> 28) {  // records are grouped by body on the host, so a warp mostly takes one case
-    case kPBuf: case kPInv: plain_body<M, 0>(vb, r, pl); break;
-    case kPAnd2: case kPNand2: case kPOr2: case kPNor2: plain_body<M, 1>(vb, r, pl); break;
-    case kPXor2: case kPXnor2: plain_body<M, 2>(vb, r, pl); break;
-    case kPAnd3: case kPNand3: case kPOr3: case kPNor3: plain_body<M, 3>(vb, r, pl); break;
-    case kPXor3: case kPXnor3: plain_body<M, 4>(vb, r, pl); break;
-    default: break;  // kPNop
+  // Records are grouped by body on the host, so a warp mostly takes one
+  // path.  A two-level tree of range tests on the class code costs fewer
+  // instructions per record than a switch over the classes.
+  const uint32_t cls = r.y >> 28;
+  if (cls >= kPAnd3) {
+    if (cls >= kPXor3) {
+      if (cls <= kPXnor3) plain_body<M, 4>(vb, r, pl);  // else kPNop
+    } else {
+      plain_body<M, 3>(vb, r, pl);
+    }
+  } else if (cls >= kPAnd2) {
+    if (cls >= kPXor2)
+      plain_body<M, 2>(vb, r, pl);
+    else
+      plain_body<M, 1>(vb, r, pl);
+  } else {
+    plain_body<M, 0>(vb, r, pl);
   }
 }
 
@@ -547,24 +557,22 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
       const uint32_t staged = min(desc.w, k.rec_buf) * 16u;
       const uint32_t np = desc.y, n = desc.y + desc.z;
       const uint32_t wide0 = (np + 1) / 2 * 16;
-      for (uint32_t p = my_off; p < n; p += nth) {
-        if (p < np) {
-          const uint32_t byte = p * 8;
-          uint2 r;
-          if (byte < staged)
-            r = *reinterpret_cast<const uint2*>(sb + byte);
-          else
-            r = *reinterpret_cast<const uint2*>(gb + byte);
-          plain_dispatch<M>(vb, r, pl);
-        } else {
-          const uint32_t byte = wide0 + (p - np) * 16;
-          uint4 q;
-          if (byte < staged)
-            q = *reinterpret_cast<const uint4*>(sb + byte);
-          else
-            q = *reinterpret_cast<const uint4*>(gb + byte);
-          gate_dispatch<M>(vals, q, pl, v.good + (uint64_t)q.w * 32 + w0, pacc);
-        }
+      // Plain records from the staging buffer, then the rest of the plain
+      // part from global memory, then the wide records: three loops
+      // without a per-record choice of source cost fewer instructions than
+      // one loop that picks the source and the record kind per position.
+      const uint32_t ns = min(np, staged / 8u);
+      uint32_t p = my_off;
+      for (; p < ns; p += nth) plain_dispatch<M>(vb, *reinterpret_cast<const uint2*>(sb + (size_t)p * 8), pl);
+      for (; p < np; p += nth) plain_dispatch<M>(vb, *reinterpret_cast<const uint2*>(gb + (size_t)p * 8), pl);
+      for (; p < n; p += nth) {
+        const uint32_t byte = wide0 + (p - np) * 16;
+        uint4 q;
+        if (byte < staged)
+          q = *reinterpret_cast<const uint4*>(sb + byte);
+        else
+          q = *reinterpret_cast<const uint4*>(gb + byte);
+        gate_dispatch<M>(vals, q, pl, v.good + (uint64_t)q.w * 32 + w0, pacc);
       }
     }
     if (__syncthreads_or(!ok)) {
@@ -588,8 +596,10 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
   return true;
 }
 
+// Register caps: the CTA sizes up to sweep_max_threads(M) fit the register
+// file, and 56 at M = 2 lets three 384-thread CTAs share an SM.
 template <int M>
-__global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(SweepArgs a) {
+__global__ void __maxnreg__(M >= 8 ? 120 : (M >= 4 ? 72 : (M >= 2 ? 56 : 64))) k_sweep(SweepArgs a) {
   extern __shared__ __align__(16) uint64_t vals[];  // [max_live][M] | recbuf[2][rec_buf]
   __shared__ unsigned long long acc[M];
   __shared__ __align__(8) uint64_t bars[3];
@@ -623,7 +633,7 @@ __global__ void __launch_bounds__(M >= 8 ? 512 : (M >= 4 ? 768 : 1024)) k_sweep(
 // circuit fields come from the kernel parameters: the compiler keeps the
 // pointers in uniform registers, as for k_sweep.
 template <int M>
-__global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : 64))
+__global__ void __maxnreg__(M >= 8 ? 96 : (M >= 4 ? 72 : (M >= 2 ? 56 : 64)))
     k_sweep_batch(const __grid_constant__ BatchSweepParams p) {
   extern __shared__ __align__(16) uint64_t vals[];
   __shared__ unsigned long long acc[M];
