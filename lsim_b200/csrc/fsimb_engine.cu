@@ -209,7 +209,6 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     sa.list = d_tune_list.as<uint32_t>();
     sa.wait_ns = kWaitLimitNs;
     sa.n_list = (uint32_t)list.size();
-    sa.subtiles = kTileWords / M;
     sa.max_gate_level = plan.max_gate_level;
     sa.N = N;
     sa.good = d_good.as<uint64_t>();
@@ -218,7 +217,7 @@ void fsimb_handle::tune_shape(cudaStream_t s, const std::vector<uint32_t>& width
     sa.vals_bytes = vals;
     sa.rec_buf = rec_buf;
     sa.err = d_err.as<int>();
-    const int nb = (int)std::min<uint64_t>((uint64_t)n_sms * got, (uint64_t)sa.n_list * sa.subtiles);
+    const int nb = (int)std::min<uint64_t>((uint64_t)n_sms * got, (uint64_t)sa.n_list * (kTileWords / M));
     // an untimed run of the first candidate warms the GPU up; then the
     // fastest of two timed runs counts
     float ms = 1e30f;
@@ -494,7 +493,6 @@ void fsimb_handle::run(const fsimb_opts* opts) {
         wa.inj = d_inj.as<InjRec>();
         wa.list = sw_list;
         wa.n_list = n_sw;
-        wa.subtiles = subtiles;
         wa.max_gate_level = plan.max_gate_level;
         wa.N = N;
         wa.good = good_t;
@@ -515,7 +513,6 @@ void fsimb_handle::run(const fsimb_opts* opts) {
         sa.inj = d_inj.as<InjRec>();
         sa.list = sw_list;
         sa.n_list = n_sw;
-        sa.subtiles = subtiles;
         sa.max_gate_level = plan.max_gate_level;
         sa.N = N;
         sa.good = good_t;

@@ -609,15 +609,16 @@ __global__ void __maxnreg__(M >= 8 ? 120 : (M >= 4 ? 72 : (M >= 2 ? 56 : 64))) k
                     (a.wait_test && blockIdx.x == 0) ? 1u : 0u);
   const SweepView v{a.blob, a.lvl, a.level, a.li_off, a.li, a.fi_off, a.fi_idx, a.type, a.good,
                     a.max_gate_level};
-  const uint32_t n_items = a.n_list * a.subtiles;
+  constexpr uint32_t subtiles = kTileWords / M;
+  const uint32_t n_items = a.n_list * subtiles;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(a.queue, 1);
     __syncthreads();
     const uint32_t item = (uint32_t)s_item;
     __syncthreads();  // s_item is rewritten for the next item only after all have read it
     if (item >= n_items) return;
-    const uint32_t li = item / a.subtiles;
-    const uint32_t w0 = (item % a.subtiles) * M;
+    const uint32_t li = item / subtiles;
+    const uint32_t w0 = (item % subtiles) * M;
     const uint32_t si = a.list ? a.list[li] : li;
     if (!sweep_item<M>(k, v, a.inj[si], w0, a.out + (uint64_t)si * 32)) {
       if (threadIdx.x == 0) atomicExch(a.err, 1);
@@ -682,15 +683,16 @@ __global__ void __launch_bounds__(256) k_sweep_wide(SweepWideArgs a) {
   uint64_t* gv = a.gvals + (size_t)blockIdx.x * a.N * M;
   const uint32_t tid = threadIdx.x, nth = blockDim.x;
   const uint32_t m = tid % M, step = nth / M;
-  const uint32_t n_items = a.n_list * a.subtiles;
+  constexpr uint32_t subtiles = kTileWords / M;
+  const uint32_t n_items = a.n_list * subtiles;
   for (;;) {
     if (tid == 0) s_item = atomicAdd(a.queue, 1);
     __syncthreads();
     const uint32_t item = s_item;
     __syncthreads();
     if (item >= n_items) return;
-    const uint32_t li = item / a.subtiles;
-    const uint32_t w0 = (item % a.subtiles) * M;
+    const uint32_t li = item / subtiles;
+    const uint32_t w0 = (item % subtiles) * M;
     const uint32_t si = a.list ? a.list[li] : li;
     const InjRec inj = a.inj[si];
     const uint32_t x = inj.elem;

@@ -33,7 +33,6 @@ struct SweepArgs {
   const InjRec* inj;
   const uint32_t* list;    // sweep indices to run (nullptr: 0..n_list-1)
   uint32_t n_list;
-  uint32_t subtiles;       // 32 / M
   uint32_t max_gate_level;
   uint32_t N;
   const uint64_t* good;    // this tile: [N][32]
@@ -57,7 +56,6 @@ struct SweepWideArgs {
   const InjRec* inj;
   const uint32_t* list;      // sweep indices to run (nullptr: 0..n_list-1)
   uint32_t n_list;
-  uint32_t subtiles;         // 32 / M
   uint32_t max_gate_level;
   uint32_t N;
   const uint64_t* good;      // this tile: [N][32]
