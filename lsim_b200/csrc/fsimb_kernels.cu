@@ -288,23 +288,20 @@ __device__ __forceinline__ void plain_body(char* vb, const uint2 r, int pl) {
 template <int M>
 __device__ __forceinline__ void plain_dispatch(char* vb, const uint2 r, int pl) {
   // Records are grouped by body on the host, so a warp mostly takes one
-  // path.  A two-level tree of range tests on the class code costs fewer
-  // instructions per record than a switch over the classes.
+  // path.  A chain of unsigned range tests on the class code, the
+  // three-input AND family first, costs fewer instructions per record than
+  // a switch over the classes.
   const uint32_t cls = r.y >> 28;
-  if (cls >= kPAnd3) {
-    if (cls >= kPXor3) {
-      if (cls <= kPXnor3) plain_body<M, 4>(vb, r, pl);  // else kPNop
-    } else {
-      plain_body<M, 3>(vb, r, pl);
-    }
-  } else if (cls >= kPAnd2) {
-    if (cls >= kPXor2)
-      plain_body<M, 2>(vb, r, pl);
-    else
-      plain_body<M, 1>(vb, r, pl);
-  } else {
+  if (cls - kPAnd3 < 4u)
+    plain_body<M, 3>(vb, r, pl);
+  else if (cls < kPAnd2)
     plain_body<M, 0>(vb, r, pl);
-  }
+  else if (cls - kPAnd2 < 4u)
+    plain_body<M, 1>(vb, r, pl);
+  else if (cls - kPXor3 < 2u)
+    plain_body<M, 4>(vb, r, pl);
+  else if (cls - kPXor2 < 2u)
+    plain_body<M, 2>(vb, r, pl);  // else kPNop
 }
 
 // ---- wide records (PO drivers, MUX, four inputs): runtime type and masks
@@ -426,8 +423,8 @@ struct SweepCta {
   uint64_t* bars;     // [3] mbarriers: two staging buffers, one for the wait test
   unsigned long long* acc;
   uint32_t rec_buf;   // 16-byte units per staging buffer
-  uint32_t phase;     // bit b: next phase parity of staging barrier b
-  uint32_t issued;    // bit b: a copy into buffer b has not been waited for yet
+  uint32_t uses;      // levels staged and consumed so far: use u goes through
+                      // buffer u & 1 and completes that barrier's phase u >> 1
   uint64_t wait_ns;   // limit of one wait
   uint32_t test_stall;
 };
@@ -441,8 +438,7 @@ __device__ __forceinline__ void sweep_cta_init(SweepCta& k, uint64_t* vals, uint
   k.bars = bars;
   k.acc = acc;
   k.rec_buf = rec_buf;
-  k.phase = 0;
-  k.issued = 0;
+  k.uses = 0;
   k.wait_ns = wait_ns;
   k.test_stall = test_stall;
   if (threadIdx.x == 0) {
@@ -462,12 +458,12 @@ __device__ __forceinline__ void sweep_stage(SweepCta& k, const SweepView& v, uin
   bulk_load(k.recbuf + (size_t)b * k.rec_buf, v.blob + d.x, n * 16u, &k.bars[b]);
 }
 
-// Error path: thread 0 waits (bounded) for the copies still in flight into
-// this CTA's shared memory, so none lands after the CTA has exited.
-__device__ __forceinline__ void sweep_drain(SweepCta& k) {
+// Error path: thread 0 waits (bounded) for the n copies still in flight
+// into this CTA's shared memory (uses u, u + 1, ...), so none lands after
+// the CTA has exited.  A copy already waited for passes at once.
+__device__ __forceinline__ void sweep_drain(SweepCta& k, uint32_t u, uint32_t n) {
   if (threadIdx.x == 0)
-    for (int b = 0; b < 2; ++b)
-      if ((k.issued >> b) & 1u) mbar_wait(&k.bars[b], (k.phase >> b) & 1u, k.wait_ns);
+    for (uint32_t i = 0; i < n; ++i) mbar_wait(&k.bars[(u + i) & 1u], ((u + i) >> 1) & 1u, k.wait_ns);
   __syncthreads();
 }
 
@@ -490,12 +486,10 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
   const uint32_t x = inj.elem;
   const uint32_t L0 = v.level[x] + 1;
   if (tid < M) k.acc[tid] = 0ull;
-  if (L0 <= Lmax) {
-    if (tid == 0) {
-      sweep_stage(k, v, L0, 0);
-      if (L0 + 1 <= Lmax) sweep_stage(k, v, L0 + 1, 1);
-    }
-    k.issued = (L0 + 1 <= Lmax) ? 3u : 1u;
+  const uint32_t n_out = L0 > Lmax ? 0u : (L0 + 1 <= Lmax ? 2u : 1u);  // copies issued ahead
+  if (tid == 0) {
+    if (n_out > 0) sweep_stage(k, v, L0, (int)(k.uses & 1u));
+    if (n_out > 1) sweep_stage(k, v, L0 + 1, (int)((k.uses + 1) & 1u));
   }
   bool ok = true;
   if (k.test_stall) {
@@ -537,7 +531,7 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
   if (tid < M && (inj.mode & kInjReachesPo))
     k.acc[tid] = inj_value(v, inj, w0 + tid) ^ v.good[(uint64_t)x * 32 + w0 + tid];
   if (__syncthreads_or(!ok)) {
-    sweep_drain(k);
+    sweep_drain(k, k.uses, n_out);
     return false;
   }
   PoAcc<M> pacc;
@@ -546,12 +540,11 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
 #pragma unroll
     for (int q = 0; q < VC; ++q) pacc[c][q] = 0ull;
   for (uint32_t L = L0; L <= Lmax; ++L) {
-    const int b = (int)((L - L0) & 1u);
+    const uint32_t u = k.uses;
+    const int b = (int)(u & 1u);
     const uint4 desc = v.lvl[L];  // issued before the wait, used after it
-    ok = mbar_wait(&k.bars[b], (k.phase >> b) & 1u, k.wait_ns);
+    ok = mbar_wait(&k.bars[b], (u >> 1) & 1u, k.wait_ns);
     if (ok) {
-      k.phase ^= 1u << b;
-      k.issued &= ~(1u << b);
       const char* sb = reinterpret_cast<const char*>(k.recbuf + (size_t)b * k.rec_buf);
       const char* gb = reinterpret_cast<const char*>(v.blob + desc.x);
       const uint32_t staged = min(desc.w, k.rec_buf) * 16u;
@@ -576,13 +569,11 @@ __device__ __forceinline__ bool sweep_item(SweepCta& k, const SweepView& v, cons
       }
     }
     if (__syncthreads_or(!ok)) {
-      sweep_drain(k);
+      sweep_drain(k, u, L + 1 <= Lmax ? 2u : 1u);
       return false;
     }
-    if (L + 2 <= Lmax) {
-      if (tid == 0) sweep_stage(k, v, L + 2, b);
-      k.issued |= 1u << b;
-    }
+    k.uses = u + 1;
+    if (L + 2 <= Lmax && tid == 0) sweep_stage(k, v, L + 2, b);
   }
 #pragma unroll
   for (int c = 0; c < C; ++c) {
