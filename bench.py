@@ -37,6 +37,8 @@ every gate output, 1,024-16,384 patterns) run as one batch (fsimb_batch_*,
 CUDA graph, autotuned sweep shape) against the same 256 circuits run one
 after another through the plain per-circuit path, both with inputs resident
 (value) and with every input copied from host memory each step (e2e).
+--gates LO,HI changes the gate-count range (e.g. 500,5000 for many circuits
+that are each too small to fill the GPU).
 
 --workload c5 times the serving configuration: 32 resident circuits
 (gen.serve_configs: 1,000-500,000 gates), requests of 1,000-100,000 faults
@@ -484,7 +486,8 @@ def _rooflines(launch_s, alg_bytes, st, clk):
 
 def run_batch(args):
     """Batched configuration: one batch of 256 circuits against 256 plain runs."""
-    print(json.dumps(batch_measure(args.circuits, args.steps, args.warmup)), flush=True)
+    lo, hi = (int(x) for x in args.gates.split(","))
+    print(json.dumps(batch_measure(args.circuits, args.steps, args.warmup, gates=(lo, hi))), flush=True)
 
 
 def batch_summary(n_circuits, steps=2):
@@ -499,13 +502,13 @@ def batch_summary(n_circuits, steps=2):
             "clocks": m["clocks"]}
 
 
-def batch_measure(n_circuits, steps, warmup, full=True):
+def batch_measure(n_circuits, steps, warmup, full=True, gates=(500, 50000)):
     import torch
     from lsim_b200 import Batch, Simulator, gen
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    cfgs = gen.batch_configs(n_circuits, seed=0)
+    cfgs = gen.batch_configs(n_circuits, seed=0, gates=gates)
     t0 = time.perf_counter()
     ws = [gen.generate(**c) for c in cfgs]
     gen_s = time.perf_counter() - t0
@@ -795,6 +798,8 @@ def main():
                          "default) or its part of the fault list (strong scaling)")
     ap.add_argument("--circuits", type=int, default=256,
                     help="circuits for --workload c4 (default 256) or c5 (default 32)")
+    ap.add_argument("--gates", default="500,50000",
+                    help="--workload c4: gate-count range of the circuits, log-uniform")
     ap.add_argument("--requests", type=int, default=200, help="requests for --workload c5")
     ap.add_argument("--rates", type=float, nargs="*", default=[0.5, 1.0, 2.0, 4.0],
                     help="--workload c5 Poisson rates, as fractions of the plain path's capacity")
